@@ -1,0 +1,186 @@
+/* tara2d_gpu.h -- C ABI of the B200 (sm_100a) pseudo-spectral RHS + time-step
+ * path of TARA2D.
+ *
+ * Two layers:
+ *
+ * 1. Drop-in entry points with the reference's Fortran calling convention
+ *    (gfortran mangling: lowercase name + '_', every argument by reference,
+ *    arrays are the caller's column-major complex(8) (Nh,Ny) buffers in host
+ *    memory, Nh = Nx/2+1).  Linking the library in place of the reference's
+ *    objects makes the drivers' `call derive2coh(...)` etc. run on the GPU.
+ *    Physical parameters are read from the COMMON /comm/ block exactly as the
+ *    reference subroutines read it (this library defines `comm_` with default
+ *    visibility, so a Fortran program's own COMMON block takes precedence).
+ *    They return nothing (like the Fortran subroutines); the status of the
+ *    last call is available from tara_legacy_status().
+ *
+ * 2. A session API (bind(C) style, explicit parameters, int status) that
+ *    keeps the spectral state resident in HBM and advances it many steps per
+ *    call; host arrays are copied only when the caller asks for them.
+ *
+ * Array convention for every double* "field" argument: interleaved
+ * (re, im) pairs of a Fortran complex(8) (Nh,Ny) array, i.e. element
+ * (i,j) (1-based) at 2*((i-1) + Nh*(j-1)).
+ *
+ * Threading: a session is not re-entrant; use one host thread per session.
+ * All sessions of a process share the current CUDA device.
+ */
+#ifndef TARA2D_GPU_H
+#define TARA2D_GPU_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define TARA_OK 0
+#define TARA_EINVAL (-1)       /* bad argument (size, pointer, model, stepper) */
+#define TARA_ECUDA (-2)        /* a CUDA runtime call failed (see tara_last_error) */
+#define TARA_ENAN (-3)         /* a non-finite value was found by a check */
+#define TARA_ETIMEOUT (-4)     /* a bounded device wait ran out */
+#define TARA_ENOMEM (-5)       /* device allocation failed */
+#define TARA_EUNSUPPORTED (-6) /* grid size or mode not built */
+
+/* ---- models ------------------------------------------------------------ */
+#define TARA_MODEL_COH 1 /* compressible isothermal hydro (nk, ukx, uky): derive2coh */
+#define TARA_MODEL_COM 2 /* compressible MHD (rho, rho_ux, rho_uy, E, Bx, By): derive2com */
+#define TARA_MODEL_CSH 3 /* incompressible vorticity (omega): derive2csh */
+#define TARA_MODEL_CSS 4 /* screened vorticity (omega): derive2css */
+
+#define TARA_FP64 0 /* FFTs, products and state in double precision */
+#define TARA_FP32 1 /* FFTs, products and state in single precision (FP64-accurate tables) */
+
+#define TARA_STEP_AB2 0   /* Adams-Bashforth 2 (src/ab2coh.f95, src/ab2com.f95) */
+#define TARA_STEP_RK4 1   /* classical RK4 of the coupled system (new) */
+#define TARA_STEP_EULER 2 /* forward Euler (src/euler2coh.f95) */
+
+/* Physical parameters.  Lx, Ly are the box lengths as the drivers hold them
+ * after `Lx = Lx*pi` (src/main2coh.f95:102); kx = 2*pi*(i-1)/Lx. */
+typedef struct {
+  double Lx, Ly, pi, dt;
+  double mux, muy, ms, CS;            /* hydro: COMMON /comm/ of src/main2coh.f95:29 */
+  double spheat, mu, mu_0, eta, kf, A; /* MHD: COMMON /comm/ of src/main2com.f95:43 (+CS, ms) */
+  double nu, alpha, lambda;           /* vorticity models */
+  int fix_curlB; /* 0: curl B as the reference builds it (src/derive2com.f95:186-187), 1: corrected */
+  int reserved[7];
+} tara_params;
+
+typedef struct tara_session tara_session;
+
+/* ---- session API -------------------------------------------------------
+ * Replaces the time loops of src/main2coh.f95:266-316 and
+ * src/main2com.f95:352-423 (derive + stepper + copy-back per step). */
+
+/* Nx, Ny in {16,32,64,128,256,384,512,1024,2048,4096}. */
+int tara_open(tara_session** out, int model, int Nx, int Ny, int precision, const tara_params* p);
+int tara_close(tara_session* s);
+int tara_set_params(tara_session* s, const tara_params* p);
+/* Number of fields of the session's model (3, 6, 1, 1). */
+int tara_num_fields(const tara_session* s);
+/* State <-> host, reference layout.  `fields` holds tara_num_fields pointers. */
+int tara_set_state(tara_session* s, const double* const* fields);
+int tara_get_state(tara_session* s, double* const* fields);
+/* AB2 history (the *_dt_old arrays of the drivers); zero after tara_open. */
+int tara_set_history(tara_session* s, const double* const* fields);
+int tara_get_history(tara_session* s, double* const* fields);
+/* Right-hand side of the current state (what derive2coh/derive2com return). */
+int tara_rhs(tara_session* s, double* const* out);
+/* Advance nsteps; asynchronous on the session's stream. */
+int tara_step(tara_session* s, int stepper, int nsteps);
+int tara_synchronize(tara_session* s);
+/* Advance nsteps and return their device time (CUDA events on the session
+ * stream, synchronised on both sides). */
+int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms);
+/* Kernel launches one step of the given stepper issues. */
+int tara_launches_per_step(const tara_session* s, int stepper);
+/* Sticky error of the session (first failure), TARA_OK if none. */
+int tara_status(const tara_session* s);
+/* Description of the last error of the calling thread ("" if none). */
+const char* tara_last_error(void);
+
+/* Explicit-parameter RHS / stepper calls on host arrays (the bind(C)
+ * entry points an iso_c_binding shim calls).  Each copies in, computes on
+ * the GPU and copies out; the grid context is cached between calls. */
+int tara_derive2coh(const tara_params* p, int Nx, int Ny, const double* nk, const double* ukx,
+                    const double* uky, double* dn_dt, double* dux_dt, double* duy_dt);
+int tara_derive2com(const tara_params* p, int Nx, int Ny, const double* const* state6,
+                    double* const* rhs6);
+
+/* ---- drop-in Fortran entry points (reference signatures) ---------------- */
+/* src/derive2coh.f95:6-7 */
+void derive2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* nk, double* ukx, double* uky, double* dn_dt_old,
+                 double* dux_dt_old, double* duy_dt_old, double* dn_dt_new, double* dux_dt_new,
+                 double* duy_dt_new);
+/* src/ab2coh.f95:5-6 */
+void ab2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+             const double* time, double* nk, double* ukx, double* uky, double* nk_new,
+             double* ukx_new, double* uky_new, double* dn_dt_old, double* dux_dt_old,
+             double* duy_dt_old, double* dn_dt_new, double* dux_dt_new, double* duy_dt_new);
+/* src/euler2coh.f95:6 */
+void euler2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                const double* time, double* nk, double* ukx, double* uky, double* nk_new,
+                double* ukx_new, double* uky_new, double* dn_dt, double* dux_dt, double* duy_dt);
+/* src/pcnk2coh.f95:6, src/pcukx2coh.f95:6, src/pcuky2coh.f95:6 */
+void pc_nk2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                const double* time, double* nk, double* nk_new, double* ukx, double* uky,
+                double* dn_dt, double* dux_dt, double* duy_dt);
+void pc_ukx2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* nk, double* ukx, double* ukx_new, double* uky,
+                 double* dn_dt, double* dux_dt, double* duy_dt);
+void pc_uky2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* nk, double* ukx, double* uky, double* uky_new,
+                 double* dn_dt, double* dux_dt, double* duy_dt);
+/* src/rk4nk2coh.f95:6, src/rk4ukx2coh.f95:6, src/rk4uky2coh.f95:6 */
+void rk4_nk2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* nk, double* nk_new, double* ukx, double* uky,
+                 double* dn_dt, double* dux_dt, double* duy_dt);
+void rk4_ukx2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                  const double* time, double* nk, double* ukx, double* ukx_new, double* uky,
+                  double* dn_dt, double* dux_dt, double* duy_dt);
+void rk4_uky2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                  const double* time, double* nk, double* ukx, double* uky, double* uky_new,
+                  double* dn_dt, double* dux_dt, double* duy_dt);
+/* src/derive2com.f95:6-8 (derivatives interleaved old/new per field) */
+void derive2com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* rho_k, double* rho_ux_k, double* rho_uy_k,
+                 double* E_k, double* Bx_k, double* By_k, double* d_rho_k_dt_old,
+                 double* d_rho_k_dt_new, double* d_rho_ux_k_dt_old, double* d_rho_ux_k_dt_new,
+                 double* d_rho_uy_k_dt_old, double* d_rho_uy_k_dt_new, double* d_E_k_dt_old,
+                 double* d_E_k_dt_new, double* d_Bx_k_dt_old, double* d_Bx_k_dt_new,
+                 double* d_By_k_dt_old, double* d_By_k_dt_new);
+/* src/ab2com.f95:6-9 */
+void ab2com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+             const double* time, double* rho_k, double* rho_ux_k, double* rho_uy_k, double* E_k,
+             double* Bx_k, double* By_k, double* rho_k_new, double* rho_ux_k_new,
+             double* rho_uy_k_new, double* E_k_new, double* Bx_k_new, double* By_k_new,
+             double* d_rho_k_dt_old, double* d_rho_k_dt_new, double* d_rho_ux_k_dt_old,
+             double* d_rho_ux_k_dt_new, double* d_rho_uy_k_dt_old, double* d_rho_uy_k_dt_new,
+             double* d_E_k_dt_old, double* d_E_k_dt_new, double* d_Bx_k_dt_old,
+             double* d_Bx_k_dt_new, double* d_By_k_dt_old, double* d_By_k_dt_new);
+
+/* Status of the last drop-in call of the calling thread. */
+int tara_legacy_status(void);
+/* Semantics of pc_*2coh_ / rk4_*2coh_:
+ *   TARA_LEGACY_REFERENCE (default): what the reference computes -- every
+ *     stage reads the unchanged argument derivative, so the update equals
+ *     (predict+correct)*dt/2 resp. dt/6*(k1+2k2+2k3+k4) with all k equal
+ *     (src/pcnk2coh.f95:31, src/rk4nk2coh.f95:33-54).  The reference's
+ *     inner derive2coh calls write only subroutine-local arrays and are not
+ *     repeated.
+ *   TARA_LEGACY_CORRECT: stage derivatives are recomputed (other fields
+ *     frozen), and the last RK4 stage is taken at dt. */
+#define TARA_LEGACY_REFERENCE 0
+#define TARA_LEGACY_CORRECT 1
+int tara_set_legacy_mode(int mode);
+
+/* COMMON /comm/ storage used by the drop-in entry points (11 doubles:
+ * hydro units read Lx,Ly,mux,muy,ms,CS,dt; MHD units read
+ * Lx,Ly,spheat,mu,ms,CS,mu_0,eta,dt,kf,A). */
+extern double comm_[16];
+
+#ifdef __cplusplus
+}
+#endif
+#endif

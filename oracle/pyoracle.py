@@ -1,0 +1,246 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: the oracle is the checker for the CUDA path, never
+part of it.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg import this module.
+
+Array convention: a Fortran ``complex(8) (Nh,Ny)`` array is a C-contiguous
+numpy ``complex128`` array of shape ``(Ny, Nh)`` (index ``[j, i]``); a Fortran
+``real(8) (Nx,Ny)`` array is ``float64`` of shape ``(Ny, Nx)``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+_lib = None
+
+
+class CohParams(C.Structure):
+    """COMMON /comm/ of the hydro units (src/main2coh.f95:29)."""
+    _fields_ = [(n, C.c_double) for n in ("Lx", "Ly", "mux", "muy", "ms", "CS", "dt")]
+
+
+class ComParams(C.Structure):
+    """COMMON /comm/ of the MHD units (src/main2com.f95:43) + defect switch."""
+    _fields_ = [(n, C.c_double) for n in
+                ("Lx", "Ly", "spheat", "mu", "ms", "CS", "mu_0", "eta", "dt", "kf", "A")] + \
+               [("fix_curlB", C.c_int)]
+
+
+def build() -> None:
+    """Build the oracle (and, with the reference checkout present, its FFTW)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        i, d = C.c_int, C.c_double
+        L = _lib
+        L.ora_derive2coh.argtypes = [i, i, i, d, d, C.POINTER(CohParams), P, P, P, P, P, P]
+        L.ora_ab2coh.argtypes = [i, i, i, C.POINTER(CohParams)] + [P] * 12
+        L.ora_euler2coh.argtypes = [i, i, i, C.POINTER(CohParams)] + [P] * 9
+        L.ora_pc2coh.argtypes = [i, i, i, i, d, d, C.POINTER(CohParams)] + [P] * 7
+        L.ora_rk42coh.argtypes = [i, i, i, i, d, d, C.POINTER(CohParams)] + [P] * 7
+        L.ora_rk4coh.argtypes = [i, i, i, d, d, C.POINTER(CohParams), P, P, P]
+        L.ora_derive2com.argtypes = [i, i, i, d, d, C.POINTER(ComParams)] + [P] * 12
+        L.ora_ab2com.argtypes = [i, i, i, C.POINTER(ComParams), P, P, P, P]
+        L.ora_rk4com.argtypes = [i, i, i, d, d, C.POINTER(ComParams), P]
+        L.ora_derive2csh.argtypes = [i, i, i, d, d, P, P]
+        L.ora_ab2csh.argtypes = [i, i, i, d, P, P, P, P]
+        L.ora_derive2css.argtypes = [i, i, i, d, d, d, d, d, d, P, P]
+        L.ora_ab2css.argtypes = [i, i, i, d, P, P, P, P]
+        L.ora_r2c_2d.argtypes = [i, i, P, P]
+        L.ora_c2r_2d.argtypes = [i, i, P, P]
+        L.ora_run_coh.argtypes = [i, i, d, C.POINTER(CohParams), i, i, P, P, P, P, P, P]
+        L.ora_run_com.argtypes = [i, i, d, C.POINTER(ComParams), i, i, P, P]
+        L.ora_diag_com.argtypes = [i, i, d, C.POINTER(ComParams), P, P]
+        L.ora_diag_coh.argtypes = [i, i, d, C.POINTER(CohParams), P, P, P, P]
+        L.ora_set_threads.argtypes = [i]
+        L.ora_get_threads.restype = i
+    return _lib
+
+
+PI = 3.14159265358979323846
+
+
+def _p(a: np.ndarray):
+    assert a.flags.c_contiguous
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _cz(shape):
+    return np.zeros(shape, dtype=np.complex128)
+
+
+def _ptr_array(arrs):
+    arr = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    return arr
+
+
+def set_threads(n: int) -> None:
+    lib().ora_set_threads(int(n))
+
+
+def r2c_2d(a: np.ndarray) -> np.ndarray:
+    Ny, Nx = a.shape
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    out = _cz((Ny, Nx // 2 + 1))
+    lib().ora_r2c_2d(Nx, Ny, _p(a), _p(out))
+    return out
+
+
+def c2r_2d(X: np.ndarray, Nx: int) -> np.ndarray:
+    Ny = X.shape[0]
+    X = np.ascontiguousarray(X, dtype=np.complex128)
+    out = np.zeros((Ny, Nx), dtype=np.float64)
+    lib().ora_c2r_2d(Nx, Ny, _p(X), _p(out))
+    return out
+
+
+def derive2coh(Nx, Ny, P: CohParams, nk, ukx, uky, pi=PI, time=0.0):
+    Nh = Nx // 2 + 1
+    ins = [np.ascontiguousarray(a, dtype=np.complex128) for a in (nk, ukx, uky)]
+    outs = [_cz((Ny, Nh)) for _ in range(3)]
+    lib().ora_derive2coh(Nx, Ny, Nh, pi, time, C.byref(P), *[_p(a) for a in ins], *[_p(a) for a in outs])
+    return outs
+
+
+def ab2coh(Nx, Ny, P: CohParams, state, d_old, d_new):
+    Nh = Nx // 2 + 1
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    do = [np.ascontiguousarray(a, dtype=np.complex128) for a in d_old]
+    dn = [np.ascontiguousarray(a, dtype=np.complex128) for a in d_new]
+    out = [_cz((Ny, Nh)) for _ in range(3)]
+    lib().ora_ab2coh(Nx, Ny, Nh, C.byref(P), *[_p(a) for a in st], *[_p(a) for a in out],
+                     *[_p(a) for a in do], *[_p(a) for a in dn])
+    return out
+
+
+def euler2coh(Nx, Ny, P: CohParams, state, d):
+    Nh = Nx // 2 + 1
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    dd = [np.ascontiguousarray(a, dtype=np.complex128) for a in d]
+    out = [_cz((Ny, Nh)) for _ in range(3)]
+    lib().ora_euler2coh(Nx, Ny, Nh, C.byref(P), *[_p(a) for a in st], *[_p(a) for a in out],
+                        *[_p(a) for a in dd])
+    return out
+
+
+def pc2coh(which, Nx, Ny, P, state, d, pi=PI, time=0.0):
+    Nh = Nx // 2 + 1
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    dd = [np.ascontiguousarray(a, dtype=np.complex128) for a in d]
+    out = _cz((Ny, Nh))
+    lib().ora_pc2coh(which, Nx, Ny, Nh, pi, time, C.byref(P), *[_p(a) for a in st], _p(out),
+                     *[_p(a) for a in dd])
+    return out
+
+
+def rk42coh(which, Nx, Ny, P, state, d, pi=PI, time=0.0):
+    Nh = Nx // 2 + 1
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    dd = [np.ascontiguousarray(a, dtype=np.complex128) for a in d]
+    out = _cz((Ny, Nh))
+    lib().ora_rk42coh(which, Nx, Ny, Nh, pi, time, C.byref(P), *[_p(a) for a in st], _p(out),
+                      *[_p(a) for a in dd])
+    return out
+
+
+def rk4coh(Nx, Ny, P, state, pi=PI, time=0.0):
+    Nh = Nx // 2 + 1
+    st = [np.array(a, dtype=np.complex128, order="C") for a in state]
+    lib().ora_rk4coh(Nx, Ny, Nh, pi, time, C.byref(P), *[_p(a) for a in st])
+    return st
+
+
+def derive2com(Nx, Ny, P: ComParams, state, pi=PI, time=0.0):
+    Nh = Nx // 2 + 1
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    outs = [_cz((Ny, Nh)) for _ in range(6)]
+    lib().ora_derive2com(Nx, Ny, Nh, pi, time, C.byref(P), *[_p(a) for a in st], *[_p(a) for a in outs])
+    return outs
+
+
+def ab2com(Nx, Ny, P: ComParams, state, d_old, d_new):
+    Nh = Nx // 2 + 1
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    do = [np.ascontiguousarray(a, dtype=np.complex128) for a in d_old]
+    dn = [np.ascontiguousarray(a, dtype=np.complex128) for a in d_new]
+    out = [_cz((Ny, Nh)) for _ in range(6)]
+    lib().ora_ab2com(Nx, Ny, Nh, C.byref(P), _ptr_array(st), _ptr_array(out), _ptr_array(do), _ptr_array(dn))
+    return out
+
+
+def rk4com(Nx, Ny, P: ComParams, state, pi=PI, time=0.0):
+    Nh = Nx // 2 + 1
+    st = [np.array(a, dtype=np.complex128, order="C") for a in state]
+    lib().ora_rk4com(Nx, Ny, Nh, pi, time, C.byref(P), _ptr_array(st))
+    return st
+
+
+def derive2csh(Nx, Ny, nu, omegak, time=0.0):
+    Nh = Nx // 2 + 1
+    w = np.ascontiguousarray(omegak, dtype=np.complex128)
+    out = _cz((Ny, Nh))
+    lib().ora_derive2csh(Nx, Ny, Nh, nu, time, _p(w), _p(out))
+    return out
+
+
+def derive2css(Nx, Ny, alpha, nu, Lx, Ly, lam, omegak, time=0.0):
+    Nh = Nx // 2 + 1
+    w = np.ascontiguousarray(omegak, dtype=np.complex128)
+    out = _cz((Ny, Nh))
+    lib().ora_derive2css(Nx, Ny, Nh, alpha, nu, time, Lx, Ly, lam, _p(w), _p(out))
+    return out
+
+
+def ab2csh(Nx, Ny, dt, w, d_old, d_new):
+    Nh = Nx // 2 + 1
+    a = [np.ascontiguousarray(x, dtype=np.complex128) for x in (w, d_old, d_new)]
+    out = _cz((Ny, Nh))
+    lib().ora_ab2csh(Nx, Ny, Nh, dt, _p(a[0]), _p(out), _p(a[1]), _p(a[2]))
+    return out
+
+
+def run_coh(Nx, Ny, P: CohParams, stepper, nsteps, state, d_old=None, pi=PI):
+    Nh = Nx // 2 + 1
+    st = [np.array(a, dtype=np.complex128, order="C") for a in state]
+    do = [np.array(a, dtype=np.complex128, order="C") for a in d_old] if d_old is not None else \
+        [_cz((Ny, Nh)) for _ in range(3)]
+    lib().ora_run_coh(Nx, Ny, pi, C.byref(P), stepper, nsteps, *[_p(a) for a in st], *[_p(a) for a in do])
+    return st, do
+
+
+def run_com(Nx, Ny, P: ComParams, stepper, nsteps, state, d_old=None, pi=PI):
+    Nh = Nx // 2 + 1
+    st = [np.array(a, dtype=np.complex128, order="C") for a in state]
+    do = [np.array(a, dtype=np.complex128, order="C") for a in d_old] if d_old is not None else \
+        [_cz((Ny, Nh)) for _ in range(6)]
+    lib().ora_run_com(Nx, Ny, pi, C.byref(P), stepper, nsteps, _ptr_array(st), _ptr_array(do))
+    return st, do
+
+
+def diag_com(Nx, Ny, P: ComParams, state, pi=PI):
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    out = np.zeros(6)
+    lib().ora_diag_com(Nx, Ny, pi, C.byref(P), _ptr_array(st), _p(out))
+    return out
+
+
+def diag_coh(Nx, Ny, P: CohParams, state, pi=PI):
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    out = np.zeros(6)
+    lib().ora_diag_coh(Nx, Ny, pi, C.byref(P), *[_p(a) for a in st], _p(out))
+    return out

@@ -1,0 +1,223 @@
+"""tara2d_b200 -- B200 (sm_100a) pseudo-spectral RHS + time-step path of TARA2D.
+
+The compute path is the CUDA shared library ``_lib/libtara2d_b200.so`` (C ABI
+in ``include/tara2d_gpu.h``).  This module is a thin ctypes binding with the
+same array convention as the reference's Fortran: a ``complex(8) (Nh,Ny)``
+array is a C-contiguous numpy ``complex128`` array of shape ``(Ny, Nh)``.
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+usable, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import initial  # noqa: F401  (seeded initial conditions)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libtara2d_b200.so")
+
+OK, EINVAL, ECUDA, ENAN, ETIMEOUT, ENOMEM, EUNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
+MODEL_COH, MODEL_COM, MODEL_CSH, MODEL_CSS = 1, 2, 3, 4
+FP64, FP32 = 0, 1
+STEP_AB2, STEP_RK4, STEP_EULER = 0, 1, 2
+LEGACY_REFERENCE, LEGACY_CORRECT = 0, 1
+SUPPORTED_N = (16, 32, 64, 128, 256, 384, 512, 1024, 2048, 4096)
+NFIELDS = {MODEL_COH: 3, MODEL_COM: 6, MODEL_CSH: 1, MODEL_CSS: 1}
+PI = 3.14159265358979323846
+
+
+class TaraError(RuntimeError):
+    pass
+
+
+class Params(C.Structure):
+    """tara_params (include/tara2d_gpu.h)."""
+    _fields_ = [(n, C.c_double) for n in
+                ("Lx", "Ly", "pi", "dt", "mux", "muy", "ms", "CS", "spheat", "mu", "mu_0", "eta",
+                 "kf", "A", "nu", "alpha", "lambda_")] + \
+               [("fix_curlB", C.c_int), ("reserved", C.c_int * 7)]
+
+    @classmethod
+    def make(cls, **kw) -> "Params":
+        p = cls()
+        p.Lx = p.Ly = 2.0 * PI
+        p.pi = PI
+        for k, v in kw.items():
+            setattr(p, "lambda_" if k == "lambda" else k, v)
+        return p
+
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise TaraError(f"CUDA library not built: {LIB_PATH} (run python -m tara2d_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        P, I, D = C.c_void_p, C.c_int, C.c_double
+        PP = C.POINTER(C.c_void_p)
+        L.tara_last_error.restype = C.c_char_p
+        L.tara_open.argtypes = [C.POINTER(C.c_void_p), I, I, I, I, C.POINTER(Params)]
+        L.tara_close.argtypes = [P]
+        L.tara_set_params.argtypes = [P, C.POINTER(Params)]
+        L.tara_num_fields.argtypes = [P]
+        for n in ("tara_set_state", "tara_get_state", "tara_set_history", "tara_get_history", "tara_rhs"):
+            getattr(L, n).argtypes = [P, PP]
+        L.tara_step.argtypes = [P, I, I]
+        L.tara_synchronize.argtypes = [P]
+        L.tara_time_steps.argtypes = [P, I, I, C.POINTER(C.c_float)]
+        L.tara_launches_per_step.argtypes = [P, I]
+        L.tara_status.argtypes = [P]
+        L.tara_derive2coh.argtypes = [C.POINTER(Params), I, I, P, P, P, P, P, P]
+        L.tara_derive2com.argtypes = [C.POINTER(Params), I, I, PP, PP]
+        L.tara_set_legacy_mode.argtypes = [I]
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().tara_last_error().decode()
+
+
+def check(status: int, what: str = "") -> None:
+    if status != OK:
+        raise TaraError(f"{what} failed with status {status}: {last_error()}")
+
+
+def _ptrs(arrs):
+    return (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+class Session:
+    """A grid whose spectral state stays in HBM (tara_open ... tara_close)."""
+
+    def __init__(self, model: int, Nx: int, Ny: int, params: Params, precision: int = FP64):
+        self.model, self.Nx, self.Ny, self.precision = model, Nx, Ny, precision
+        self.Nh = Nx // 2 + 1
+        self.nf = NFIELDS[model]
+        self.params = params
+        h = C.c_void_p()
+        check(lib().tara_open(C.byref(h), model, Nx, Ny, precision, C.byref(params)), "tara_open")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().tara_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _fields_in(self, fields):
+        arrs = [np.ascontiguousarray(f, dtype=np.complex128) for f in fields]
+        assert len(arrs) == self.nf and all(a.shape == (self.Ny, self.Nh) for a in arrs)
+        return arrs
+
+    def _fields_out(self):
+        return [np.zeros((self.Ny, self.Nh), dtype=np.complex128) for _ in range(self.nf)]
+
+    def set_params(self, params: Params) -> None:
+        self.params = params
+        check(lib().tara_set_params(self._h, C.byref(params)), "tara_set_params")
+
+    def set_state(self, fields) -> None:
+        a = self._fields_in(fields)
+        check(lib().tara_set_state(self._h, _ptrs(a)), "tara_set_state")
+
+    def get_state(self):
+        out = self._fields_out()
+        check(lib().tara_get_state(self._h, _ptrs(out)), "tara_get_state")
+        return out
+
+    def set_history(self, fields) -> None:
+        a = self._fields_in(fields)
+        check(lib().tara_set_history(self._h, _ptrs(a)), "tara_set_history")
+
+    def get_history(self):
+        out = self._fields_out()
+        check(lib().tara_get_history(self._h, _ptrs(out)), "tara_get_history")
+        return out
+
+    def rhs(self):
+        out = self._fields_out()
+        check(lib().tara_rhs(self._h, _ptrs(out)), "tara_rhs")
+        return out
+
+    def step(self, stepper: int, nsteps: int) -> None:
+        check(lib().tara_step(self._h, stepper, nsteps), "tara_step")
+
+    def synchronize(self) -> None:
+        check(lib().tara_synchronize(self._h), "tara_synchronize")
+
+    def time_steps(self, stepper: int, nsteps: int) -> float:
+        ms = C.c_float()
+        check(lib().tara_time_steps(self._h, stepper, nsteps, C.byref(ms)), "tara_time_steps")
+        return ms.value
+
+    def launches_per_step(self, stepper: int) -> int:
+        return lib().tara_launches_per_step(self._h, stepper)
+
+    @property
+    def status(self) -> int:
+        return lib().tara_status(self._h)
+
+
+# ---- drop-in Fortran entry points (reference calling convention) ----------
+_COH = ("Lx", "Ly", "mux", "muy", "ms", "CS", "dt")
+_COM = ("Lx", "Ly", "spheat", "mu", "ms", "CS", "mu_0", "eta", "dt", "kf", "A")
+
+
+def set_comm(values) -> None:
+    """Write the COMMON /comm/ block the drop-in entry points read."""
+    comm = (C.c_double * 16).in_dll(lib(), "comm_")
+    for i, v in enumerate(values):
+        comm[i] = float(v)
+
+
+def comm_coh(p: Params):
+    return [getattr(p, n) for n in _COH]
+
+
+def comm_com(p: Params):
+    return [getattr(p, n) for n in _COM]
+
+
+def _i32(v):
+    return C.byref(C.c_int32(v))
+
+
+def _d(v):
+    return C.byref(C.c_double(v))
+
+
+def legacy_call(name: str, Nx: int, Ny: int, pi: float, time: float, arrays) -> int:
+    """Call a drop-in entry point (e.g. 'derive2coh_') with Fortran-style
+    arguments: Nx, Ny, Nh, pi, time by reference, then the arrays in the
+    reference's order.  Returns tara_legacy_status()."""
+    fn = getattr(lib(), name)
+    args = [_i32(Nx), _i32(Ny), _i32(Nx // 2 + 1), _d(pi), _d(time)]
+    for a in arrays:
+        assert a.dtype == np.complex128 and a.flags.c_contiguous
+        args.append(C.c_void_p(a.ctypes.data))
+    fn(*args)
+    return lib().tara_legacy_status()
+
+
+def set_legacy_mode(mode: int) -> None:
+    check(lib().tara_set_legacy_mode(mode), "tara_set_legacy_mode")

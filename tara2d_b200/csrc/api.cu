@@ -1,0 +1,673 @@
+// C ABI: sessions (state resident in HBM) and the drop-in Fortran entry
+// points with the reference's calling convention.
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+#include "models.h"
+
+using namespace tara;
+
+extern "C" {
+double comm_[16] = {0};
+}
+
+namespace {
+
+// host complex(8) (Nh,Ny) <-> device [Ny][ld] Cx<float>
+__global__ void k_f64_to_f32(const double2* __restrict__ src, Cx<float>* dst, int Nh, int ld, int Ny) {
+  size_t n = (size_t)Nh * Ny;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    int j = (int)(q / Nh), i = (int)(q % Nh);
+    double2 v = src[q];
+    dst[(size_t)j * ld + i] = cx<float>((float)v.x, (float)v.y);
+  }
+}
+__global__ void k_f32_to_f64(const Cx<float>* src, double2* __restrict__ dst, int Nh, int ld, int Ny) {
+  size_t n = (size_t)Nh * Ny;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    int j = (int)(q / Nh), i = (int)(q % Nh);
+    Cx<float> v = src[(size_t)j * ld + i];
+    dst[q] = make_double2((double)v.x, (double)v.y);
+  }
+}
+
+// elementwise steppers on [Ny][ld] fields
+enum : int { EW_AB2 = 0, EW_EULER = 1, EW_PC_REF = 2, EW_RK4_REF = 3, EW_AXPY = 4, EW_PC = 5 };
+template <class T> struct EwArgs {
+  int mode, nf, Nh, ld, Ny;
+  T dt, alpha;
+  const Cx<T>* u[6];
+  const Cx<T>* d1[6];
+  const Cx<T>* d2[6];
+  Cx<T>* out[6];
+};
+// Operation order: ab2coh.f95:22, euler2coh.f95:104, pcnk2coh.f95:32, rk4nk2coh.f95:54.
+template <class T>
+__global__ void k_elementwise(const EwArgs<T> a) {
+  const size_t n = (size_t)a.Nh * a.Ny;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const size_t o = (q / a.Nh) * a.ld + (q % a.Nh);
+    for (int f = 0; f < a.nf; f++) {
+      const Cx<T> u = a.u[f][o], d = a.d1[f][o];
+      Cx<T> r;
+      switch (a.mode) {
+        case EW_AB2: r = u + rmul(a.dt, rmul((T)1.5, d) - rmul((T)0.5, a.d2[f][o])); break;
+        case EW_EULER: r = u + rmul(a.dt, d); break;
+        case EW_PC_REF: case EW_PC: {
+          const Cx<T> s = d + (a.mode == EW_PC ? a.d2[f][o] : d);
+          r = u + cx<T>(s.x * a.dt / (T)2, s.y * a.dt / (T)2);
+          break;
+        }
+        case EW_RK4_REF: {
+          const Cx<T> s = ((d + rmul((T)2, d)) + rmul((T)2, d)) + d;
+          r = u + rmul(a.alpha, s);  // alpha = dt/6
+          break;
+        }
+        default: r = u + rmul(a.alpha, d); break;  // EW_AXPY
+      }
+      a.out[f][o] = r;
+    }
+  }
+}
+
+int nfields_of(int model) {
+  switch (model) {
+    case TARA_MODEL_COH: return 3;
+    case TARA_MODEL_COM: return 6;
+    case TARA_MODEL_CSH: case TARA_MODEL_CSS: return 1;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+struct tara_session {
+  int model = 0, precision = 0, Nx = 0, Ny = 0, Nh = 0, nf = 0;
+  tara_params p{};
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int status = TARA_OK;
+  virtual ~tara_session() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (st) cudaStreamDestroy(st);
+  }
+  virtual int init() = 0;
+  virtual int apply_params() = 0;
+  virtual int set_fields(int which, const double* const* h) = 0;  // which: 0 state, 1 history
+  virtual int get_fields(int which, double* const* h) = 0;
+  virtual int rhs_to_host(double* const* out) = 0;
+  virtual int step(int stepper, int n) = 0;
+  virtual int launches(int stepper) const = 0;
+  int fail_if(int s) {
+    if (s != TARA_OK && status == TARA_OK) status = s;
+    return s;
+  }
+  // elementwise stepper on host fields (drop-in ab2/euler/pc/rk4 entry points);
+  // nfld fields, each out = stepper(u, d1, d2)
+  virtual int elementwise(int mode, int nfld, const double* const* u, const double* const* d1,
+                          const double* const* d2, double* const* out) = 0;
+  // per-field PC / RK4 with the other hydro fields frozen (TARA_LEGACY_CORRECT)
+  virtual int frozen_field_step(bool rk4, int which, const double* const* f, const double* d,
+                                double* out) = 0;
+};
+
+namespace {
+
+template <class T>
+struct SessionT : tara_session {
+  Grid<T> g;
+  FieldPool<T> u, dold, acc, us, tmp;
+  FieldPool<double> stage;  // FP32 sessions: FP64 staging of host transfers
+  CohWork<T> cw;
+  ComWork<T> mw;
+  VortWork<T> vw;
+  CohParamsT<T> cohp{};
+  ComParamsT<T> comp{};
+  VortParamsT<T> vortp{};
+
+  ~SessionT() override {
+    if (st) cudaStreamSynchronize(st);
+    g.release(); u.release(); dold.release(); acc.release(); us.release(); tmp.release();
+    stage.release(); cw.release(); mw.release(); vw.release();
+  }
+
+  int init() override {
+    TARA_TRY(g.init(Nx, Ny, p.Lx, p.Ly, p.pi, st));
+    TARA_TRY(u.alloc(g, nf, st));
+    TARA_TRY(dold.alloc(g, nf, st));
+    TARA_TRY(acc.alloc(g, nf, st));
+    TARA_TRY(us.alloc(g, nf, st));
+    TARA_TRY(tmp.alloc(g, nf, st));
+    if (sizeof(T) != sizeof(double)) {
+      // staging as complex128 [Ny][Nh] (host layout, no pitch)
+      stage.elems = (size_t)Nh * Ny;
+      stage.count = 1;
+      if (cudaMalloc(&stage.base, stage.elems * sizeof(Cx<double>)) != cudaSuccess) {
+        stage.base = nullptr;
+        set_error("cudaMalloc of staging buffer failed");
+        return TARA_ENOMEM;
+      }
+    }
+    switch (model) {
+      case TARA_MODEL_COH: TARA_TRY(cw.alloc(g, st)); break;
+      case TARA_MODEL_COM: TARA_TRY(mw.alloc(g, st)); break;
+      default: TARA_TRY(vw.alloc(g, st)); break;
+    }
+    TARA_TRY(apply_params());
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+
+  int apply_params() override {
+    if (p.Lx != g.Lx || p.Ly != g.Ly || p.pi != g.pi) {
+      // wavenumber tables depend on Lx, Ly and pi
+      TARA_CUDA_TRY(cudaStreamSynchronize(st));
+      g.release();
+      TARA_TRY(g.init(Nx, Ny, p.Lx, p.Ly, p.pi, st));
+    }
+    cohp.mux = (T)p.mux;
+    cohp.muy = (T)p.muy;
+    cohp.cs2 = (T)(p.CS * p.CS);
+    comp.mu = (T)p.mu;
+    comp.eta = (T)p.eta;
+    comp.cs2 = (T)(p.CS * p.CS);
+    comp.kf = (T)p.kf;
+    comp.A = (T)p.A;
+    comp.fix_curlB = p.fix_curlB;
+    vortp.nu = (T)p.nu;
+    vortp.alpha = (T)p.alpha;
+    vortp.lambda = (T)p.lambda;
+    vortp.screened = model == TARA_MODEL_CSS;
+    return TARA_OK;
+  }
+
+  FieldPool<T>& pool(int which) { return which == 0 ? u : dold; }
+
+  int h2d(const double* h, Cx<T>* d) {
+    if (!h) { set_error("null host field pointer"); return TARA_EINVAL; }
+    if constexpr (sizeof(T) == sizeof(double)) {
+      TARA_CUDA_TRY(cudaMemcpy2DAsync(d, g.ld * sizeof(Cx<T>), h, Nh * sizeof(Cx<double>),
+                                      Nh * sizeof(Cx<double>), Ny, cudaMemcpyHostToDevice, st));
+    } else {
+      TARA_CUDA_TRY(cudaMemcpyAsync(stage.base, h, stage.elems * sizeof(Cx<double>),
+                                    cudaMemcpyHostToDevice, st));
+      k_f64_to_f32<<<512, 256, 0, st>>>(reinterpret_cast<const double2*>(stage.base),
+                                        reinterpret_cast<Cx<float>*>(d), Nh, g.ld, Ny);
+      TARA_CUDA_TRY(cudaGetLastError());
+    }
+    return TARA_OK;
+  }
+  int d2h(const Cx<T>* d, double* h) {
+    if (!h) { set_error("null host field pointer"); return TARA_EINVAL; }
+    if constexpr (sizeof(T) == sizeof(double)) {
+      TARA_CUDA_TRY(cudaMemcpy2DAsync(h, Nh * sizeof(Cx<double>), d, g.ld * sizeof(Cx<T>),
+                                      Nh * sizeof(Cx<double>), Ny, cudaMemcpyDeviceToHost, st));
+    } else {
+      k_f32_to_f64<<<512, 256, 0, st>>>(reinterpret_cast<const Cx<float>*>(d),
+                                        reinterpret_cast<double2*>(stage.base), Nh, g.ld, Ny);
+      TARA_CUDA_TRY(cudaGetLastError());
+      TARA_CUDA_TRY(cudaMemcpyAsync(h, stage.base, stage.elems * sizeof(Cx<double>),
+                                    cudaMemcpyDeviceToHost, st));
+    }
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+
+  int set_fields(int which, const double* const* h) override {
+    if (!h) { set_error("null field array"); return TARA_EINVAL; }
+    for (int f = 0; f < nf; f++) TARA_TRY(h2d(h[f], pool(which)[f]));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+  int get_fields(int which, double* const* h) override {
+    if (!h) { set_error("null field array"); return TARA_EINVAL; }
+    for (int f = 0; f < nf; f++) TARA_TRY(d2h(pool(which)[f], h[f]));
+    return TARA_OK;
+  }
+
+  int rhs(Cx<T>* const* in, const StepArgs<T>& s) {
+    switch (model) {
+      case TARA_MODEL_COH: return coh_rhs(g, cw, cohp, in, s, st);
+      case TARA_MODEL_COM: return com_rhs(g, mw, comp, in, s, st);
+      default: return vort_rhs(g, vw, vortp, in, s, st);
+    }
+  }
+  StepArgs<T> base_args(int mode) {
+    StepArgs<T> s{};
+    s.mode = mode;
+    s.dt = (T)p.dt;
+    for (int f = 0; f < nf; f++) {
+      s.out[f] = tmp[f];
+      s.u[f] = u[f];
+      s.dold[f] = dold[f];
+      s.acc[f] = acc[f];
+      s.us[f] = us[f];
+    }
+    return s;
+  }
+  int rhs_to_host(double* const* out) override {
+    if (!out) { set_error("null field array"); return TARA_EINVAL; }
+    Cx<T>* in[6];
+    for (int f = 0; f < nf; f++) in[f] = u[f];
+    TARA_TRY(rhs(in, base_args(STEP_RHS)));
+    for (int f = 0; f < nf; f++) TARA_TRY(d2h(tmp[f], out[f]));
+    return TARA_OK;
+  }
+  int step(int stepper, int n) override {
+    Cx<T>* in_u[6];
+    Cx<T>* in_s[6];
+    for (int f = 0; f < nf; f++) { in_u[f] = u[f]; in_s[f] = us[f]; }
+    for (int t = 0; t < n; t++) {
+      if (stepper == TARA_STEP_AB2) {
+        TARA_TRY(rhs(in_u, base_args(STEP_AB2)));
+      } else if (stepper == TARA_STEP_EULER) {
+        TARA_TRY(rhs(in_u, base_args(STEP_EULER)));
+      } else if (stepper == TARA_STEP_RK4) {
+        // classical RK4; weights and stage offsets as in the oracle:
+        // acc = u + (w dt/6) k1 ; us = u + (c dt) k ; u = acc + (dt/6) k4
+        const double w[4] = {1.0, 2.0, 2.0, 1.0}, c[3] = {0.5, 0.5, 1.0};
+        for (int s = 0; s < 4; s++) {
+          StepArgs<T> a = base_args(STEP_RK4);
+          a.stage = s;
+          a.wa = (T)(w[s] * p.dt / 6.0);
+          a.cs = s < 3 ? (T)(c[s] * p.dt) : (T)0;
+          TARA_TRY(rhs(s == 0 ? in_u : in_s, a));
+        }
+      } else {
+        set_error("unknown stepper");
+        return TARA_EINVAL;
+      }
+    }
+    return TARA_OK;
+  }
+  void ew(int mode, int nfld, Cx<T>* const* u, Cx<T>* const* d1, Cx<T>* const* d2,
+          Cx<T>* const* out, T alpha) {
+    EwArgs<T> a{};
+    a.mode = mode; a.nf = nfld; a.Nh = Nh; a.ld = g.ld; a.Ny = Ny;
+    a.dt = (T)p.dt; a.alpha = alpha;
+    for (int f = 0; f < nfld; f++) { a.u[f] = u[f]; a.d1[f] = d1[f]; a.d2[f] = d2[f]; a.out[f] = out[f]; }
+    k_elementwise<T><<<592, 256, 0, st>>>(a);
+  }
+  int elementwise(int mode, int nfld, const double* const* u, const double* const* d1,
+                  const double* const* d2, double* const* out) override {
+    if (!u || !d1 || !d2 || !out) { set_error("null field array"); return TARA_EINVAL; }
+    Cx<T>* du[6];
+    Cx<T>* dd1[6];
+    Cx<T>* dd2[6];
+    for (int f = 0; f < nfld; f++) {
+      du[f] = acc[f]; dd1[f] = tmp[f]; dd2[f] = us[f];
+      TARA_TRY(h2d(u[f], du[f]));
+      TARA_TRY(h2d(d1[f], dd1[f]));
+      if (mode == EW_AB2) TARA_TRY(h2d(d2[f], dd2[f]));
+    }
+    ew(mode, nfld, du, dd1, dd2, du, (T)(p.dt / 6.0));
+    TARA_CUDA_TRY(cudaGetLastError());
+    for (int f = 0; f < nfld; f++) TARA_TRY(d2h(du[f], out[f]));
+    return TARA_OK;
+  }
+  int frozen_field_step(bool rk4, int w, const double* const* f, const double* d, double* out) override {
+    if (model != TARA_MODEL_COH || w < 0 || w > 2) { set_error("bad field"); return TARA_EINVAL; }
+    for (int q = 0; q < 3; q++) TARA_TRY(h2d(f[q], u[q]));
+    TARA_TRY(h2d(d, dold[w]));  // k1
+    const size_t fb = g.field_bytes();
+    Cx<T>* in_s[6] = {us[0], us[1], us[2]};
+    Cx<T>* uw[1] = {u[w]};
+    Cx<T>* usw[1] = {us[w]};
+    Cx<T>* accw[1] = {acc[w]};
+    Cx<T>* kw[1] = {tmp[w]};
+    Cx<T>* k1[1] = {dold[w]};
+    for (int q = 0; q < 3; q++) TARA_CUDA_TRY(cudaMemcpyAsync(us[q], u[q], fb, cudaMemcpyDeviceToDevice, st));
+    if (!rk4) {
+      // predictor u + dt*k1, corrector with the refreshed derivative
+      ew(EW_AXPY, 1, uw, k1, k1, usw, (T)p.dt);
+      TARA_TRY(rhs(in_s, base_args(STEP_RHS)));
+      ew(EW_PC, 1, uw, k1, kw, accw, (T)0);
+    } else {
+      const double c[3] = {0.5, 0.5, 1.0}, wgt[4] = {1.0, 2.0, 2.0, 1.0};
+      ew(EW_AXPY, 1, uw, k1, k1, accw, (T)(wgt[0] * p.dt / 6.0));
+      Cx<T>* kprev[1] = {dold[w]};
+      for (int s = 0; s < 3; s++) {
+        ew(EW_AXPY, 1, uw, kprev, kprev, usw, (T)(c[s] * p.dt));
+        TARA_TRY(rhs(in_s, base_args(STEP_RHS)));
+        ew(EW_AXPY, 1, accw, kw, kw, accw, (T)(wgt[s + 1] * p.dt / 6.0));
+        kprev[0] = tmp[w];
+      }
+    }
+    TARA_CUDA_TRY(cudaGetLastError());
+    return d2h(acc[w], out);
+  }
+  int launches(int stepper) const override {
+    int per = model == TARA_MODEL_COH ? kCohLaunches : model == TARA_MODEL_COM ? kComLaunches : kVortLaunches;
+    return stepper == TARA_STEP_RK4 ? 4 * per : per;
+  }
+};
+
+tara_session* make_session(int precision) {
+  if (precision == TARA_FP32) return new SessionT<float>();
+  return new SessionT<double>();
+}
+
+thread_local int g_legacy_status = TARA_OK;
+int g_legacy_mode = TARA_LEGACY_REFERENCE;
+std::mutex g_legacy_mu;
+std::map<std::tuple<int, int, int>, std::unique_ptr<tara_session>> g_legacy;
+
+}  // namespace
+
+// ======================================================================
+// session API
+// ======================================================================
+extern "C" {
+
+const char* tara_last_error(void) { return tara::last_error(); }
+
+int tara_open(tara_session** out, int model, int Nx, int Ny, int precision, const tara_params* p) {
+  if (!out || !p) { set_error("null argument"); return TARA_EINVAL; }
+  *out = nullptr;
+  int nf = nfields_of(model);
+  if (!nf) { set_error("unknown model"); return TARA_EINVAL; }
+  if (precision != TARA_FP64 && precision != TARA_FP32) { set_error("unknown precision"); return TARA_EINVAL; }
+  if (!supported_length(Nx) || !supported_length(Ny)) {
+    set_error("grid size not supported (Nx, Ny in {16,32,64,128,256,384,512,1024,2048,4096})");
+    return TARA_EUNSUPPORTED;
+  }
+  std::unique_ptr<tara_session> s(make_session(precision));
+  s->model = model; s->precision = precision; s->Nx = Nx; s->Ny = Ny; s->Nh = Nx / 2 + 1; s->nf = nf;
+  s->p = *p;
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
+    set_error(std::string("CUDA initialisation failed: ") + cudaGetErrorString(cudaGetLastError()));
+    return TARA_ECUDA;
+  }
+  int r = s->init();
+  if (r != TARA_OK) return r;
+  *out = s.release();
+  return TARA_OK;
+}
+
+int tara_close(tara_session* s) {
+  if (!s) return TARA_EINVAL;
+  delete s;
+  return TARA_OK;
+}
+
+int tara_set_params(tara_session* s, const tara_params* p) {
+  if (!s || !p) return TARA_EINVAL;
+  s->p = *p;
+  return s->fail_if(s->apply_params());
+}
+
+int tara_num_fields(const tara_session* s) { return s ? s->nf : 0; }
+
+int tara_set_state(tara_session* s, const double* const* f) { return s ? s->fail_if(s->set_fields(0, f)) : TARA_EINVAL; }
+int tara_get_state(tara_session* s, double* const* f) { return s ? s->fail_if(s->get_fields(0, f)) : TARA_EINVAL; }
+int tara_set_history(tara_session* s, const double* const* f) { return s ? s->fail_if(s->set_fields(1, f)) : TARA_EINVAL; }
+int tara_get_history(tara_session* s, double* const* f) { return s ? s->fail_if(s->get_fields(1, f)) : TARA_EINVAL; }
+int tara_rhs(tara_session* s, double* const* out) { return s ? s->fail_if(s->rhs_to_host(out)) : TARA_EINVAL; }
+
+int tara_step(tara_session* s, int stepper, int nsteps) {
+  if (!s || nsteps < 0) return TARA_EINVAL;
+  return s->fail_if(s->step(stepper, nsteps));
+}
+int tara_synchronize(tara_session* s) {
+  if (!s) return TARA_EINVAL;
+  cudaError_t e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
+    return s->fail_if(TARA_ECUDA);
+  }
+  return TARA_OK;
+}
+int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms) {
+  if (!s || !ms || nsteps < 0) return TARA_EINVAL;
+  if (cudaStreamSynchronize(s->st) != cudaSuccess) return s->fail_if(TARA_ECUDA);
+  cudaEventRecord(s->ev0, s->st);
+  int r = s->step(stepper, nsteps);
+  if (r != TARA_OK) return s->fail_if(r);
+  cudaEventRecord(s->ev1, s->st);
+  cudaError_t e = cudaEventSynchronize(s->ev1);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaEventSynchronize: ") + cudaGetErrorString(e));
+    return s->fail_if(TARA_ECUDA);
+  }
+  cudaEventElapsedTime(ms, s->ev0, s->ev1);
+  return TARA_OK;
+}
+int tara_launches_per_step(const tara_session* s, int stepper) { return s ? s->launches(stepper) : 0; }
+int tara_status(const tara_session* s) { return s ? s->status : TARA_EINVAL; }
+
+}  // extern "C"
+
+// ======================================================================
+// drop-in entry points
+// ======================================================================
+namespace {
+
+// Cached FP64 session per (model, Nx, Ny) for the per-call entry points.
+// Caller holds g_legacy_mu.
+tara_session* legacy_session(int model, int Nx, int Ny, const tara_params& p, int& status) {
+  auto key = std::make_tuple(model, Nx, Ny);
+  auto it = g_legacy.find(key);
+  if (it != g_legacy.end()) {
+    tara_session* s = it->second.get();
+    s->p = p;
+    status = s->apply_params();
+    return status == TARA_OK ? s : nullptr;
+  }
+  tara_session* s = nullptr;
+  status = tara_open(&s, model, Nx, Ny, TARA_FP64, &p);
+  if (status != TARA_OK) return nullptr;
+  g_legacy[key].reset(s);
+  return s;
+}
+
+tara_params coh_params_from_comm(double pi) {
+  // COMMON /comm/ Lx,Ly,mux,muy,ms,CS,dt   (src/derive2coh.f95:30)
+  tara_params p{};
+  p.Lx = comm_[0]; p.Ly = comm_[1]; p.mux = comm_[2]; p.muy = comm_[3];
+  p.ms = comm_[4]; p.CS = comm_[5]; p.dt = comm_[6]; p.pi = pi;
+  return p;
+}
+tara_params com_params_from_comm(double pi) {
+  // COMMON /comm/ Lx,Ly,spheat,mu,ms,CS,mu_0,eta,dt,kf,A   (src/derive2com.f95:48)
+  tara_params p{};
+  p.Lx = comm_[0]; p.Ly = comm_[1]; p.spheat = comm_[2]; p.mu = comm_[3]; p.ms = comm_[4];
+  p.CS = comm_[5]; p.mu_0 = comm_[6]; p.eta = comm_[7]; p.dt = comm_[8]; p.kf = comm_[9];
+  p.A = comm_[10]; p.pi = pi;
+  return p;
+}
+
+bool check_dims(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh) {
+  if (!Nx || !Ny || !Nh || *Nh != *Nx / 2 + 1) {
+    set_error("inconsistent Nx/Ny/Nh");
+    g_legacy_status = TARA_EINVAL;
+    return false;
+  }
+  return true;
+}
+
+void legacy_derive(int model, int Nx, int Ny, const tara_params& p, const double* const* in,
+                   double* const* out) {
+  std::lock_guard<std::mutex> lk(g_legacy_mu);
+  int st = TARA_OK;
+  tara_session* s = legacy_session(model, Nx, Ny, p, st);
+  if (s) st = s->set_fields(0, in);
+  if (st == TARA_OK) st = s->rhs_to_host(out);
+  g_legacy_status = st;
+}
+
+void legacy_elementwise(int model, int Nx, int Ny, const tara_params& p, int mode, int nfld,
+                        const double* const* u, const double* const* d1, const double* const* d2,
+                        double* const* out) {
+  std::lock_guard<std::mutex> lk(g_legacy_mu);
+  int st = TARA_OK;
+  tara_session* s = legacy_session(model, Nx, Ny, p, st);
+  if (s) st = s->elementwise(mode, nfld, u, d1, d2, out);
+  g_legacy_status = st;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tara_legacy_status(void) { return g_legacy_status; }
+int tara_set_legacy_mode(int mode) {
+  if (mode != TARA_LEGACY_REFERENCE && mode != TARA_LEGACY_CORRECT) return TARA_EINVAL;
+  g_legacy_mode = mode;
+  return TARA_OK;
+}
+
+int tara_derive2coh(const tara_params* p, int Nx, int Ny, const double* nk, const double* ukx,
+                    const double* uky, double* dn_dt, double* dux_dt, double* duy_dt) {
+  if (!p) return TARA_EINVAL;
+  const double* in[3] = {nk, ukx, uky};
+  double* out[3] = {dn_dt, dux_dt, duy_dt};
+  legacy_derive(TARA_MODEL_COH, Nx, Ny, *p, in, out);
+  return g_legacy_status;
+}
+int tara_derive2com(const tara_params* p, int Nx, int Ny, const double* const* state6,
+                    double* const* rhs6) {
+  if (!p || !state6 || !rhs6) return TARA_EINVAL;
+  legacy_derive(TARA_MODEL_COM, Nx, Ny, *p, state6, rhs6);
+  return g_legacy_status;
+}
+
+void derive2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* nk, double* ukx, double* uky, double* dn_dt_old,
+                 double* dux_dt_old, double* duy_dt_old, double* dn_dt_new, double* dux_dt_new,
+                 double* duy_dt_new) {
+  (void)time; (void)dn_dt_old; (void)dux_dt_old; (void)duy_dt_old;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* in[3] = {nk, ukx, uky};
+  double* out[3] = {dn_dt_new, dux_dt_new, duy_dt_new};
+  legacy_derive(TARA_MODEL_COH, *Nx, *Ny, coh_params_from_comm(*pi), in, out);
+}
+
+void ab2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+             const double* time, double* nk, double* ukx, double* uky, double* nk_new,
+             double* ukx_new, double* uky_new, double* dn_dt_old, double* dux_dt_old,
+             double* duy_dt_old, double* dn_dt_new, double* dux_dt_new, double* duy_dt_new) {
+  (void)time;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* u[3] = {nk, ukx, uky};
+  const double* dn[3] = {dn_dt_new, dux_dt_new, duy_dt_new};
+  const double* dol[3] = {dn_dt_old, dux_dt_old, duy_dt_old};
+  double* out[3] = {nk_new, ukx_new, uky_new};
+  legacy_elementwise(TARA_MODEL_COH, *Nx, *Ny, coh_params_from_comm(*pi), EW_AB2, 3, u, dn, dol, out);
+}
+
+void euler2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                const double* time, double* nk, double* ukx, double* uky, double* nk_new,
+                double* ukx_new, double* uky_new, double* dn_dt, double* dux_dt, double* duy_dt) {
+  (void)time;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* u[3] = {nk, ukx, uky};
+  const double* d[3] = {dn_dt, dux_dt, duy_dt};
+  double* out[3] = {nk_new, ukx_new, uky_new};
+  legacy_elementwise(TARA_MODEL_COH, *Nx, *Ny, coh_params_from_comm(*pi), EW_EULER, 3, u, d, d, out);
+}
+
+}  // extern "C"
+
+namespace {
+// pc_*2coh / rk4_*2coh: advance field `which` (0 nk, 1 ukx, 2 uky).
+void legacy_pc_rk4(bool rk4, int which, const int32_t* Nx, const int32_t* Ny, const int32_t* Nh,
+                   const double* pi, double* nk, double* ukx, double* uky, double* out,
+                   double* dn_dt, double* dux_dt, double* duy_dt) {
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* f[3] = {nk, ukx, uky};
+  const double* d[3] = {dn_dt, dux_dt, duy_dt};
+  tara_params p = coh_params_from_comm(*pi);
+  if (g_legacy_mode == TARA_LEGACY_REFERENCE) {
+    const double* u1[1] = {f[which]};
+    const double* d1[1] = {d[which]};
+    double* o1[1] = {out};
+    legacy_elementwise(TARA_MODEL_COH, *Nx, *Ny, p, rk4 ? EW_RK4_REF : EW_PC_REF, 1, u1, d1, d1, o1);
+    return;
+  }
+  std::lock_guard<std::mutex> lk(g_legacy_mu);
+  int st = TARA_OK;
+  tara_session* s = legacy_session(TARA_MODEL_COH, *Nx, *Ny, p, st);
+  if (s) st = s->frozen_field_step(rk4, which, f, d[which], out);
+  g_legacy_status = st;
+}
+}  // namespace
+
+extern "C" {
+void pc_nk2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                const double* time, double* nk, double* nk_new, double* ukx, double* uky,
+                double* dn_dt, double* dux_dt, double* duy_dt) {
+  (void)time;
+  legacy_pc_rk4(false, 0, Nx, Ny, Nh, pi, nk, ukx, uky, nk_new, dn_dt, dux_dt, duy_dt);
+}
+void pc_ukx2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* nk, double* ukx, double* ukx_new, double* uky,
+                 double* dn_dt, double* dux_dt, double* duy_dt) {
+  (void)time;
+  legacy_pc_rk4(false, 1, Nx, Ny, Nh, pi, nk, ukx, uky, ukx_new, dn_dt, dux_dt, duy_dt);
+}
+void pc_uky2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* nk, double* ukx, double* uky, double* uky_new,
+                 double* dn_dt, double* dux_dt, double* duy_dt) {
+  (void)time;
+  legacy_pc_rk4(false, 2, Nx, Ny, Nh, pi, nk, ukx, uky, uky_new, dn_dt, dux_dt, duy_dt);
+}
+void rk4_nk2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* nk, double* nk_new, double* ukx, double* uky,
+                 double* dn_dt, double* dux_dt, double* duy_dt) {
+  (void)time;
+  legacy_pc_rk4(true, 0, Nx, Ny, Nh, pi, nk, ukx, uky, nk_new, dn_dt, dux_dt, duy_dt);
+}
+void rk4_ukx2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                  const double* time, double* nk, double* ukx, double* ukx_new, double* uky,
+                  double* dn_dt, double* dux_dt, double* duy_dt) {
+  (void)time;
+  legacy_pc_rk4(true, 1, Nx, Ny, Nh, pi, nk, ukx, uky, ukx_new, dn_dt, dux_dt, duy_dt);
+}
+void rk4_uky2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                  const double* time, double* nk, double* ukx, double* uky, double* uky_new,
+                  double* dn_dt, double* dux_dt, double* duy_dt) {
+  (void)time;
+  legacy_pc_rk4(true, 2, Nx, Ny, Nh, pi, nk, ukx, uky, uky_new, dn_dt, dux_dt, duy_dt);
+}
+
+void derive2com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+                 const double* time, double* rho_k, double* rho_ux_k, double* rho_uy_k,
+                 double* E_k, double* Bx_k, double* By_k, double* d_rho_k_dt_old,
+                 double* d_rho_k_dt_new, double* d_rho_ux_k_dt_old, double* d_rho_ux_k_dt_new,
+                 double* d_rho_uy_k_dt_old, double* d_rho_uy_k_dt_new, double* d_E_k_dt_old,
+                 double* d_E_k_dt_new, double* d_Bx_k_dt_old, double* d_Bx_k_dt_new,
+                 double* d_By_k_dt_old, double* d_By_k_dt_new) {
+  (void)time; (void)d_rho_k_dt_old; (void)d_rho_ux_k_dt_old; (void)d_rho_uy_k_dt_old;
+  (void)d_E_k_dt_old; (void)d_Bx_k_dt_old; (void)d_By_k_dt_old;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* in[6] = {rho_k, rho_ux_k, rho_uy_k, E_k, Bx_k, By_k};
+  double* out[6] = {d_rho_k_dt_new, d_rho_ux_k_dt_new, d_rho_uy_k_dt_new, d_E_k_dt_new,
+                    d_Bx_k_dt_new, d_By_k_dt_new};
+  legacy_derive(TARA_MODEL_COM, *Nx, *Ny, com_params_from_comm(*pi), in, out);
+}
+
+void ab2com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
+             const double* time, double* rho_k, double* rho_ux_k, double* rho_uy_k, double* E_k,
+             double* Bx_k, double* By_k, double* rho_k_new, double* rho_ux_k_new,
+             double* rho_uy_k_new, double* E_k_new, double* Bx_k_new, double* By_k_new,
+             double* d_rho_k_dt_old, double* d_rho_k_dt_new, double* d_rho_ux_k_dt_old,
+             double* d_rho_ux_k_dt_new, double* d_rho_uy_k_dt_old, double* d_rho_uy_k_dt_new,
+             double* d_E_k_dt_old, double* d_E_k_dt_new, double* d_Bx_k_dt_old,
+             double* d_Bx_k_dt_new, double* d_By_k_dt_old, double* d_By_k_dt_new) {
+  (void)time;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* u[6] = {rho_k, rho_ux_k, rho_uy_k, E_k, Bx_k, By_k};
+  const double* dn[6] = {d_rho_k_dt_new, d_rho_ux_k_dt_new, d_rho_uy_k_dt_new, d_E_k_dt_new,
+                         d_Bx_k_dt_new, d_By_k_dt_new};
+  const double* dol[6] = {d_rho_k_dt_old, d_rho_ux_k_dt_old, d_rho_uy_k_dt_old, d_E_k_dt_old,
+                          d_Bx_k_dt_old, d_By_k_dt_old};
+  double* out[6] = {rho_k_new, rho_ux_k_new, rho_uy_k_new, E_k_new, Bx_k_new, By_k_new};
+  legacy_elementwise(TARA_MODEL_COM, *Nx, *Ny, com_params_from_comm(*pi), EW_AB2, 6, u, dn, dol, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,228 @@
+// Generic column kernels (inverse y pass, forward y pass + dealias + time
+// step) and the launch configurations shared by every model.
+#pragma once
+#include "spectral.cuh"
+
+namespace tara {
+
+// ------------------------------------------------------------ configurations
+// Column pass: CB adjacent kx columns per CTA, P values per thread.
+template <class T, int L> struct ColCfg { static constexpr int CB = 4, P = 16; };
+template <int L> struct ColCfg<double, L> {
+  static constexpr int P = (L == 384) ? 24 : 16;
+  static constexpr int CB = (L <= 256) ? 8 : (L <= 1024 ? 4 : 2);
+};
+template <int L> struct ColCfg<float, L> {
+  static constexpr int P = (L == 384) ? 24 : 16;
+  static constexpr int CB = (L <= 1024) ? 8 : 4;
+};
+// Row pass: P values per thread (M = Nx/2 points per row FFT).
+template <int M> struct RowCfg { static constexpr int P = 16; };
+template <> struct RowCfg<8> { static constexpr int P = 8; };
+template <> struct RowCfg<192> { static constexpr int P = 24; };
+template <> struct RowCfg<512> { static constexpr int P = 8; };
+
+#define TARA_DISPATCH_LEN(n, FN, ...)                    \
+  switch (n) {                                           \
+    case 16: FN<16>(__VA_ARGS__); break;                 \
+    case 32: FN<32>(__VA_ARGS__); break;                 \
+    case 64: FN<64>(__VA_ARGS__); break;                 \
+    case 128: FN<128>(__VA_ARGS__); break;               \
+    case 256: FN<256>(__VA_ARGS__); break;               \
+    case 384: FN<384>(__VA_ARGS__); break;               \
+    case 512: FN<512>(__VA_ARGS__); break;               \
+    case 1024: FN<1024>(__VA_ARGS__); break;             \
+    case 2048: FN<2048>(__VA_ARGS__); break;             \
+    case 4096: FN<4096>(__VA_ARGS__); break;             \
+    default: break;                                      \
+  }
+
+// ------------------------------------------------------------ multipliers
+enum : int { MUL_ONE = 0, MUL_IKY = 1, MUL_KY2 = 2 };
+
+template <class T>
+__device__ __forceinline__ Cx<T> apply_ymul(int mul, T ky, Cx<T> x) {
+  if (mul == MUL_IKY) return ikmul(ky, x);       // (0,1)*ky*x
+  if (mul == MUL_KY2) return rmul(ky * ky, x);   // ky*ky*x
+  return x;
+}
+
+// ------------------------------------------------------------ inverse y pass
+template <class T> struct ColInvJob {
+  const Cx<T>* src;
+  Cx<T>* dst;
+  int mul;
+};
+template <class T> struct ColInvArgs {
+  Tables<T> tb;
+  ColInvJob<T> job[8];
+};
+
+// blockIdx.x: tile of CB kx columns; blockIdx.y: job
+template <class T, int L, int CB, int P>
+__global__ void __launch_bounds__(CB * L / P) k_col_inv(const ColInvArgs<T> a) {
+  using F = FFTB<L, CB, P>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+  const ColInvJob<T> jb = a.job[blockIdx.y];
+  const int c0 = blockIdx.x * CB;
+  const int Nh = a.tb.Nh, ld = a.tb.ld;
+  const T* ky = a.tb.ky;
+  Cx<T> v[P];
+  fft_run<F, +1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
+    const int c = c0 + t;
+    if (c >= Nh) return cx<T>(0, 0);
+    return apply_ymul(jb.mul, __ldg(ky + i), ldg(jb.src + (size_t)i * ld + c));
+  }, SyncBlock{});
+  fft_emit<F>(threadIdx.x, v, [&](int t, int i, Cx<T> x) {
+    const int c = c0 + t;
+    if (c < Nh) st(jb.dst + (size_t)i * ld + c, x);
+  });
+}
+
+// ------------------------------------------------------------ time steppers
+enum : int { STEP_RHS = 0, STEP_AB2 = 1, STEP_EULER = 2, STEP_RK4 = 3 };
+
+template <class T> struct StepArgs {
+  int mode;
+  int stage;   // RK4 stage 0..3
+  T dt;
+  T wa;        // RK4: weight*dt/6 of this stage
+  T cs;        // RK4: c*dt of the next stage input
+  Cx<T>* out[6];  // STEP_RHS: derivative output
+  Cx<T>* u[6];    // state (AB2/Euler: updated in place; RK4: base state)
+  Cx<T>* dold[6]; // AB2 history, replaced by the new derivative
+  Cx<T>* acc[6];  // RK4 accumulator
+  Cx<T>* us[6];   // RK4 next stage input
+};
+
+// d = derivative of field f at element idx.  Operation order follows
+// src/ab2coh.f95:22 / src/ab2com.f95:69 and src/euler2coh.f95:104.
+template <class T>
+__device__ __forceinline__ void step_apply(const StepArgs<T>& s, int f, size_t idx, Cx<T> d) {
+  switch (s.mode) {
+    case STEP_RHS:
+      st(s.out[f] + idx, d);
+      break;
+    case STEP_AB2: {
+      Cx<T> old = ld(s.dold[f] + idx);
+      Cx<T> u = ld(s.u[f] + idx);
+      Cx<T> inc = rmul((T)1.5, d) - rmul((T)0.5, old);
+      st(s.u[f] + idx, u + rmul(s.dt, inc));
+      st(s.dold[f] + idx, d);
+      break;
+    }
+    case STEP_EULER: {
+      Cx<T> u = ld(s.u[f] + idx);
+      st(s.u[f] + idx, u + rmul(s.dt, d));
+      st(s.dold[f] + idx, d);
+      break;
+    }
+    default: {  // RK4
+      if (s.stage == 0) {
+        Cx<T> u = ld(s.u[f] + idx);
+        st(s.acc[f] + idx, u + rmul(s.wa, d));
+        st(s.us[f] + idx, u + rmul(s.cs, d));
+      } else if (s.stage < 3) {
+        Cx<T> u = ld(s.u[f] + idx);
+        Cx<T> a = ld(s.acc[f] + idx);
+        st(s.acc[f] + idx, a + rmul(s.wa, d));
+        st(s.us[f] + idx, u + rmul(s.cs, d));
+      } else {
+        Cx<T> a = ld(s.acc[f] + idx);
+        st(s.u[f] + idx, a + rmul(s.wa, d));
+      }
+      break;
+    }
+  }
+}
+
+// ------------------------------------------------------------ forward y pass
+// One output field per CTA row of the grid (blockIdx.y = f): forward y DFT of
+// X[f], circular 2/3 dealiasing, sign, then the stepper update.
+template <class T> struct ColFwdSimpleArgs {
+  Tables<T> tb;
+  const Cx<T>* X[6];
+  T sign[6];  // derivative = sign * dealiased transform
+  StepArgs<T> step;
+};
+
+template <class T, int L, int CB, int P>
+__global__ void __launch_bounds__(CB * L / P) k_col_fwd_simple(const ColFwdSimpleArgs<T> a) {
+  using F = FFTB<L, CB, P>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+  const int f = blockIdx.y;
+  const int c0 = blockIdx.x * CB;
+  const int Nh = a.tb.Nh, ld = a.tb.ld;
+  const Cx<T>* X = a.X[f];
+  Cx<T> v[P];
+  fft_run<F, -1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
+    const int c = c0 + t;
+    if (c >= Nh) return cx<T>(0, 0);
+    return ldg(X + (size_t)i * ld + c);
+  }, SyncBlock{});
+  const T sg = a.sign[f];
+  fft_emit<F>(threadIdx.x, v, [&](int t, int j, Cx<T> x) {
+    const int c = c0 + t;
+    if (c >= Nh) return;
+    const bool masked = c >= __ldg(a.tb.cut + j);
+    Cx<T> val = masked ? cx<T>(0, 0) : x;
+    Cx<T> d = cx<T>(sg * val.x, sg * val.y);
+    step_apply(a.step, f, (size_t)j * ld + c, d);
+  });
+}
+
+template <class T, int L>
+inline size_t col_smem_bytes() {
+  return (size_t)ColCfg<T, L>::CB * L * sizeof(Cx<T>);
+}
+
+template <class T, int L>
+inline int launch_col_inv(const ColInvArgs<T>& a, int njobs, cudaStream_t st) {
+  constexpr int CB = ColCfg<T, L>::CB, P = ColCfg<T, L>::P;
+  auto kern = k_col_inv<T, L, CB, P>;
+  const size_t smem = col_smem_bytes<T, L>();
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 grid((a.tb.Nh + CB - 1) / CB, njobs);
+  kern<<<grid, CB * L / P, smem, st>>>(a);
+  return 0;
+}
+
+template <class T, int L>
+inline int launch_col_fwd_simple(const ColFwdSimpleArgs<T>& a, int nf, cudaStream_t st) {
+  constexpr int CB = ColCfg<T, L>::CB, P = ColCfg<T, L>::P;
+  auto kern = k_col_fwd_simple<T, L, CB, P>;
+  const size_t smem = col_smem_bytes<T, L>();
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 grid((a.tb.Nh + CB - 1) / CB, nf);
+  kern<<<grid, CB * L / P, smem, st>>>(a);
+  return 0;
+}
+
+template <int L, class T>
+inline void col_inv_dispatch(const ColInvArgs<T>& a, int njobs, cudaStream_t st) {
+  launch_col_inv<T, L>(a, njobs, st);
+}
+template <int L, class T>
+inline void col_fwd_simple_dispatch(const ColFwdSimpleArgs<T>& a, int nf, cudaStream_t st) {
+  launch_col_fwd_simple<T, L>(a, nf, st);
+}
+
+template <class T>
+inline void run_col_inv(const ColInvArgs<T>& a, int njobs, cudaStream_t st) {
+  TARA_DISPATCH_LEN(a.tb.Ny, col_inv_dispatch, a, njobs, st)
+}
+template <class T>
+inline void run_col_fwd_simple(const ColFwdSimpleArgs<T>& a, int nf, cudaStream_t st) {
+  TARA_DISPATCH_LEN(a.tb.Ny, col_fwd_simple_dispatch, a, nf, st)
+}
+
+// rows per CTA for a row kernel with ntr threads per row
+inline int rows_per_cta(int ntr, int Ny, size_t smem_per_row) {
+  int rb = 1;
+  while (rb * 2 * ntr <= 64 && Ny % (rb * 2) == 0 && (rb * 2) * smem_per_row <= 96 * 1024) rb *= 2;
+  return rb;
+}
+
+}  // namespace tara

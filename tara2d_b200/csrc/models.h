@@ -1,0 +1,61 @@
+// Model RHS launchers.  Each launches the kernels of one right-hand-side
+// evaluation on `st` and hands every derivative value to the stepper
+// epilogue described by StepArgs (write it out, AB2, Euler or an RK4 stage).
+#pragma once
+#include "plan.h"
+#include "kernels.cuh"
+
+namespace tara {
+
+// ---- compressible isothermal hydro, src/derive2coh.f95 ----
+template <class T> struct CohParamsT { T mux, muy, cs2; };
+template <class T> struct CohWork {
+  FieldPool<T> H;  // 8 half-real fields: n, iky n, ux, iky ux, ky2 ux, uy, iky uy, ky2 uy
+  FieldPool<T> X;  // 3 x-transformed rows: NLn, momentum-x, momentum-y
+  int alloc(const Grid<T>& g, cudaStream_t st) {
+    int s = H.alloc(g, 8, st);
+    if (s) return s;
+    return X.alloc(g, 3, st);
+  }
+  void release() { H.release(); X.release(); }
+};
+template <class T>
+int coh_rhs(const Grid<T>& g, CohWork<T>& w, const CohParamsT<T>& p, Cx<T>* const in[3],
+            const StepArgs<T>& step, cudaStream_t st);
+constexpr int kCohLaunches = 3;
+
+// ---- compressible MHD, src/derive2com.f95 ----
+template <class T> struct ComParamsT { T mu, eta, cs2, kf, A; int fix_curlB; };
+template <class T> struct ComWork {
+  FieldPool<T> H;  // half-real: rho, rho_ux, rho_uy, E, Bx, By, d(uy)/dy, [iky Bx, ikx By]
+  FieldPool<T> X;  // x-transformed rows: ux, uy, Mxx, Mxy, Myy, Mag, Ex, Ey, EV, Fx, Fy
+  int alloc(const Grid<T>& g, cudaStream_t st) {
+    int s = H.alloc(g, 9, st);
+    if (s) return s;
+    return X.alloc(g, 11, st);
+  }
+  void release() { H.release(); X.release(); }
+};
+template <class T>
+int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* const in[6],
+            const StepArgs<T>& step, cudaStream_t st);
+constexpr int kComLaunches = 5;
+
+// ---- incompressible (screened) vorticity, src/derive2csh.f95, src/derive2css.f95 ----
+template <class T> struct VortParamsT { T nu, alpha, lambda; int screened; };
+template <class T> struct VortWork {
+  FieldPool<T> H;  // ux, uy, d omega/dx, d omega/dy (half-real)
+  FieldPool<T> X;  // u.grad omega (x-transformed)
+  int alloc(const Grid<T>& g, cudaStream_t st) {
+    int s = H.alloc(g, 4, st);
+    if (s) return s;
+    return X.alloc(g, 1, st);
+  }
+  void release() { H.release(); X.release(); }
+};
+template <class T>
+int vort_rhs(const Grid<T>& g, VortWork<T>& w, const VortParamsT<T>& p, Cx<T>* const in[1],
+             const StepArgs<T>& step, cudaStream_t st);
+constexpr int kVortLaunches = 3;
+
+}  // namespace tara

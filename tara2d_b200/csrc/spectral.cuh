@@ -1,0 +1,199 @@
+// Device building blocks of the pseudo-spectral RHS: the column (y) pass and
+// the row (x) real-FFT passes, written on top of the Stockham engine in
+// fft_core.cuh.
+//
+// Layouts on the device (one field):
+//   spectral  [Ny][ld]  Cx<T>, element (kx index i, ky index j) at j*ld + i,
+//             i < Nh = Nx/2+1, ld = Nh rounded up (128-byte rows).  This is the
+//             reference's Fortran (Nh,Ny) array with a row pitch.
+//   half-real [Ny][ld]  Cx<T>: the same array after the inverse y transform
+//             (every kx column transformed, nothing dropped yet).
+//
+// 2D c2r (reference semantics, FFTW 3.3.9 rank-geq2 rdft2):
+//   1. complex inverse DFT along y of every kx column (column pass),
+//   2. c2r along x of every row; the imaginary parts of the kx = 0 and
+//      kx = Nx/2 bins are ignored (row pass).
+// 2D r2c: r2c along x of every row, then forward DFT along y.
+#pragma once
+#include <cuda_runtime.h>
+#include "fft_core.cuh"
+
+namespace tara {
+
+// Per-grid read-only tables (device pointers).
+template <class T>
+struct Tables {
+  const Cx<T>* tw_col;   // e^{-2 pi i m/Ny},     m < Ny
+  const Cx<T>* tw_row;   // e^{-2 pi i m/(Nx/2)}, m < Nx/2
+  const Cx<T>* tw_real;  // e^{-2 pi i k/Nx},     k <= Nx/2
+  const T* kx;           // kx(i) = 2 pi i/Lx,                    i < Nh
+  const T* ky;           // ky(j) = 2 pi j/Ly or 2 pi (j-Ny)/Ly,  j < Ny
+  const int* cut;        // row j: modes with kx index >= cut[j] are dealiased
+  int Nx, Ny, Nh, ld;
+  T inv_nn;              // 1/(Nx*Ny)
+  T nn;                  // Nx*Ny
+  int nn_pow2;           // Nx*Ny is a power of two (so x*inv_nn == x/nn exactly)
+};
+
+template <class T> __device__ __forceinline__ Cx<T> ldg(const Cx<T>* p);
+template <> __device__ __forceinline__ Cx<double> ldg(const Cx<double>* p) {
+  double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  return cx<double>(v.x, v.y);
+}
+template <> __device__ __forceinline__ Cx<float> ldg(const Cx<float>* p) {
+  float2 v = __ldg(reinterpret_cast<const float2*>(p));
+  return cx<float>(v.x, v.y);
+}
+// plain (coherent) load, for buffers written earlier in the same kernel
+template <class T> __device__ __forceinline__ Cx<T> ld(const Cx<T>* p) { return *p; }
+template <class T> __device__ __forceinline__ void st(Cx<T>* p, Cx<T> v) {
+  if constexpr (sizeof(T) == 8) {
+    *reinterpret_cast<double2*>(p) = make_double2(v.x, v.y);
+  } else {
+    *reinterpret_cast<float2*>(p) = make_float2(v.x, v.y);
+  }
+}
+
+template <class T> struct TwGlobal {
+  const Cx<T>* p;
+  __device__ __forceinline__ Cx<T> operator()(int m) const { return ldg(p + m); }
+};
+
+template <class T> __device__ __forceinline__ T normalise(T x, const Tables<T>& tb) {
+  return tb.nn_pow2 ? x * tb.inv_nn : x / tb.nn;
+}
+
+// ------------------------------------------------------------------ stages
+// Generic driver of one batched FFT whose intermediate stages go through the
+// shared-memory tile `sm` (element (t, i) at sm[i*B + t]).  `pro(t, i)`
+// supplies stage-0 input (t, i); `epi(t, i, v)` consumes output (t, i).
+// All threads of the group must call it (it contains barriers via SYNC).
+template <class F, int s, class T, class SYNC>
+__device__ __forceinline__ void fft_store(Cx<T>* sm, int tid, const Cx<T>* v, SYNC sync) {
+  constexpr int R = F::Pl::R[s];
+#pragma unroll
+  for (int q = 0; q < F::P / R; q++)
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      int t, i;
+      F::template out_pos<s>(tid, q, r, t, i);
+      sm[i * F::B_ + t] = v[q * R + r];
+    }
+}
+template <class F, int s, class T>
+__device__ __forceinline__ void fft_load(const Cx<T>* sm, int tid, Cx<T>* v) {
+  constexpr int R = F::Pl::R[s];
+#pragma unroll
+  for (int q = 0; q < F::P / R; q++)
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      int t, i;
+      F::template in_pos<s>(tid, q, r, t, i);
+      v[q * R + r] = sm[i * F::B_ + t];
+    }
+}
+template <class F, int s, int DIR, class T, class TW, class SYNC>
+__device__ __forceinline__ void fft_rest(Cx<T>* sm, int tid, Cx<T>* v, const TW& tw, SYNC sync) {
+  if constexpr (s < F::S) {
+    sync();
+    fft_store<F, s - 1>(sm, tid, v, sync);
+    sync();
+    fft_load<F, s>(sm, tid, v);
+    F::template compute<s, DIR>(tid, v, tw);
+    fft_rest<F, s + 1, DIR>(sm, tid, v, tw, sync);
+  }
+}
+
+// Runs the transform; on return v[] holds the outputs of the last stage for
+// this thread, positions given by F::out_pos<S-1>.
+template <class F, int DIR, class T, class TW, class PRO, class SYNC>
+__device__ __forceinline__ void fft_run(Cx<T>* sm, int tid, Cx<T>* v, const TW& tw, PRO&& pro, SYNC sync) {
+  constexpr int R0 = F::Pl::R[0];
+#pragma unroll
+  for (int q = 0; q < F::P / R0; q++)
+#pragma unroll
+    for (int r = 0; r < R0; r++) {
+      int t, i;
+      F::template in_pos<0>(tid, q, r, t, i);
+      v[q * R0 + r] = pro(t, i);
+    }
+  F::template compute<0, DIR>(tid, v, tw);
+  fft_rest<F, 1, DIR>(sm, tid, v, tw, sync);
+}
+template <class F, class T, class EPI>
+__device__ __forceinline__ void fft_emit(int tid, const Cx<T>* v, EPI&& epi) {
+  constexpr int R = F::Pl::R[F::S - 1];
+#pragma unroll
+  for (int q = 0; q < F::P / R; q++)
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      int t, i;
+      F::template out_pos<F::S - 1>(tid, q, r, t, i);
+      epi(t, i, v[q * R + r]);
+    }
+}
+
+// BatchFFT with the batch size exposed for the smem layout.
+template <int L, int B, int P> struct FFTB : BatchFFT<L, B, P> {
+  static constexpr int B_ = B;
+};
+
+struct SyncBlock {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+// ----------------------------------------------------------- row helpers
+// Inverse real transform of one row: X[0..M] -> x[0..2M-1] (unnormalised).
+// hv(k) returns X[k] for 0 < k < M; for k = 0 and k = M only its real part
+// is used (the kx = 0 / Nyquist bins of a c2r).  On return the thread holds
+// z[n] = x[2n] + i x[2n+1] for its output positions n (RowF::out_pos).
+template <class RowF, class T, class HV>
+__device__ __forceinline__ void row_c2r(Cx<T>* xs, int lane, Cx<T>* v, const Tables<T>& tb, HV&& hv) {
+  constexpr int M = RowF::L_;
+  TwGlobal<T> tw{tb.tw_row};
+  fft_run<RowF, +1>(xs, lane, v, tw, [&](int, int i) -> Cx<T> {
+    Cx<T> A, B;
+    if (i == 0) {
+      A = cx<T>(hv(0).x, (T)0);
+      B = cx<T>(hv(M).x, (T)0);
+    } else {
+      A = hv(i);
+      B = conj(hv(M - i));
+    }
+    Cx<T> fe = A + B;
+    Cx<T> w = ldg(tb.tw_real + i);  // e^{-2 pi i i/N}
+    Cx<T> fo = cmul(A - B, conj(w));
+    return cx<T>(fe.x - fo.y, fe.y + fo.x);
+  }, SyncBlock{});
+}
+
+// Forward real transform of one row: x[0..2M-1] -> X[0..M].
+// gv(n) returns z[n] = x[2n] + i x[2n+1]; out(k, X) is called for k = 0..M
+// (X[0], X[M] real).  zs is an M-element smem buffer private to the row.
+template <class RowF, class T, class GV, class OUT>
+__device__ __forceinline__ void row_r2c(Cx<T>* zs, int lane, int ntr, Cx<T>* v, const Tables<T>& tb,
+                                        GV&& gv, OUT&& out) {
+  constexpr int M = RowF::L_;
+  TwGlobal<T> tw{tb.tw_row};
+  fft_run<RowF, -1>(zs, lane, v, tw, [&](int, int i) { return gv(i); }, SyncBlock{});
+  __syncthreads();
+  fft_emit<RowF>(lane, v, [&](int, int i, Cx<T> z) { zs[i] = z; });
+  __syncthreads();
+  for (int k = lane; k <= M; k += ntr) {
+    Cx<T> zk = zs[k == M ? 0 : k];
+    Cx<T> zm = conj(zs[k == 0 ? 0 : M - k]);
+    Cx<T> e = rmul((T)0.5, zk + zm);
+    Cx<T> d = zk - zm;
+    Cx<T> o = cx<T>((T)0.5 * d.y, (T)-0.5 * d.x);  // (zk - zm)/(2i)
+    Cx<T> w = ldg(tb.tw_real + k);
+    Cx<T> X = e + cmul(w, o);
+    if (k == 0 || k == M) X.y = (T)0;
+    out(k, X);
+  }
+}
+
+template <int L, int P> struct RowFFT : FFTB<L, 1, P> {
+  static constexpr int L_ = L;
+};
+
+}  // namespace tara

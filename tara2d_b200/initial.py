@@ -1,0 +1,116 @@
+"""Seeded initial conditions of the benchmark configurations (host side).
+
+The reference's drivers build their initial states on the host and transform
+them with FFTW r2c (src/main2coh.f95:141-222, src/main2com.f95:230-300); the
+benchmark configurations replace the reference's point-vortex / uniform-B
+profiles with seeded random-phase and Orszag-Tang states, built here with
+numpy (PCG64 via ``numpy.random.default_rng(seed)``).  The same arrays feed the
+GPU path and the CPU oracle.
+
+Arrays: real fields (Ny, Nx) float64; spectral state (Ny, Nh) complex128 =
+unnormalised r2c of the real field (the reference's convention).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PI = 3.14159265358979323846
+
+
+def grid(Nx: int, Ny: int, Lx: float = 2 * PI, Ly: float = 2 * PI):
+    """x_i = (i-1) dx, y_j = (j-1) dy (src/main2coh.f95:142-145)."""
+    x = np.arange(Nx) * (Lx / Nx)
+    y = np.arange(Ny) * (Ly / Ny)
+    return np.meshgrid(x, y)  # X[j, i], Y[j, i]
+
+
+def _kgrid_full(Nx, Ny, Lx=2 * PI, Ly=2 * PI):
+    kx = np.fft.fftfreq(Nx, d=1.0 / Nx) * (2 * PI / Lx)
+    ky = np.fft.fftfreq(Ny, d=1.0 / Ny) * (2 * PI / Ly)
+    return np.meshgrid(kx, ky)
+
+
+def r2c(a: np.ndarray) -> np.ndarray:
+    return np.fft.rfft2(a)
+
+
+def solenoidal_random(Nx, Ny, rng, spectrum, kmin=0.0, kmax=np.inf, Lx=2 * PI, Ly=2 * PI):
+    """Random-phase divergence-free (ux, uy) with shell spectrum E(k) ~ spectrum(k).
+
+    u = (d psi/dy, -d psi/dx), as the reference builds ukx = i ky psi,
+    uky = -i kx psi (src/main2coh.f95:198-200)."""
+    KX, KY = _kgrid_full(Nx, Ny, Lx, Ly)
+    K = np.sqrt(KX ** 2 + KY ** 2)
+    amp = np.zeros_like(K)
+    sel = (K > 0) & (K >= kmin) & (K <= kmax)
+    # E(k) ~ 2 pi k * k^2 |psi|^2 / 2  =>  |psi| ~ sqrt(E(k)/k^3)
+    amp[sel] = np.sqrt(spectrum(K[sel]) / K[sel] ** 3)
+    phase = rng.uniform(0.0, 2 * PI, size=K.shape)
+    psik = amp * np.exp(1j * phase)
+    psi = np.real(np.fft.ifft2(psik))
+    psik = np.fft.fft2(psi)
+    ux = np.real(np.fft.ifft2(1j * KY * psik))
+    uy = np.real(np.fft.ifft2(-1j * KX * psik))
+    return ux, uy
+
+
+def _normalise(ux, uy, energy):
+    e = 0.5 * np.mean(ux * ux + uy * uy)
+    s = np.sqrt(energy / e) if e > 0 else 0.0
+    return ux * s, uy * s
+
+
+def coh_random_phase(Nx=128, Ny=128, seed=0, k0=4.0, energy=0.5, noise=0.01):
+    """Hydro state (nk, ukx, uky): solenoidal u with E(k) ~ k^4 exp(-(k/k0)^2),
+    total energy `energy`; density 1 + noise*N(0,1)."""
+    rng = np.random.default_rng(seed)
+    ux, uy = solenoidal_random(Nx, Ny, rng, lambda k: k ** 4 * np.exp(-(k / k0) ** 2))
+    ux, uy = _normalise(ux, uy, energy)
+    n = 1.0 + noise * rng.standard_normal((Ny, Nx))
+    return [r2c(n), r2c(ux), r2c(uy)]
+
+
+def com_state(rho, ux, uy, Bx, By, CS, spheat=5.0 / 3.0):
+    """Conservative MHD state (rho, rho ux, rho uy, E, Bx, By) in k-space with
+    P = CS^2 rho and E = P/(spheat-1) + rho u^2/2 + B^2/2 (src/main2com.f95:247-255)."""
+    P = CS * CS * rho
+    E = P / (spheat - 1.0) + 0.5 * rho * (ux ** 2 + uy ** 2) + 0.5 * (Bx ** 2 + By ** 2)
+    return [r2c(rho), r2c(rho * ux), r2c(rho * uy), r2c(E), r2c(Bx), r2c(By)]
+
+
+def com_orszag_tang(Nx=1024, Ny=1024, seed=0, amp=1e-3, kmin=8.0, kmax=16.0, CS=100.0):
+    """u = (-sin y, sin x), B = (-sin y, sin 2x), rho = 1, plus seeded
+    random-phase solenoidal perturbations of rms `amp` on kmin <= |k| <= kmax
+    in u and in B."""
+    rng = np.random.default_rng(seed)
+    X, Y = grid(Nx, Ny)
+    ux, uy = -np.sin(Y), np.sin(X)
+    Bx, By = -np.sin(Y), np.sin(2.0 * X)
+    flat = lambda k: np.ones_like(k) * k  # E(k) ~ k : equal energy per mode
+    pux, puy = solenoidal_random(Nx, Ny, rng, flat, kmin, kmax)
+    pbx, pby = solenoidal_random(Nx, Ny, rng, flat, kmin, kmax)
+    for a, b in ((pux, puy), (pbx, pby)):
+        rms = np.sqrt(np.mean(a * a + b * b))
+        if rms > 0:
+            a *= amp / rms
+            b *= amp / rms
+    rho = np.ones((Ny, Nx))
+    return com_state(rho, ux + pux, uy + puy, Bx + pbx, By + pby, CS)
+
+
+def com_random_phase(Nx, Ny, seed=0, k0=6.0, ekin=0.5, emag=0.5, CS=100.0):
+    """MHD state with random-phase u and B, both E(k) ~ k^4 exp(-(k/k0)^2)."""
+    rng = np.random.default_rng(seed)
+    spec = lambda k: k ** 4 * np.exp(-(k / k0) ** 2)
+    ux, uy = _normalise(*solenoidal_random(Nx, Ny, rng, spec), ekin)
+    bx, by = _normalise(*solenoidal_random(Nx, Ny, rng, spec), emag)
+    return com_state(np.ones((Ny, Nx)), ux, uy, bx, by, CS)
+
+
+def vorticity_random_phase(Nx, Ny, seed=0, k0=4.0, energy=0.5):
+    """omega_k = i kx uy_k - i ky ux_k of a random-phase solenoidal field."""
+    rng = np.random.default_rng(seed)
+    ux, uy = _normalise(*solenoidal_random(Nx, Ny, rng, lambda k: k ** 4 * np.exp(-(k / k0) ** 2)), energy)
+    KX, KY = _kgrid_full(Nx, Ny)
+    w = np.real(np.fft.ifft2(1j * KX * np.fft.fft2(uy) - 1j * KY * np.fft.fft2(ux)))
+    return [r2c(w)]
