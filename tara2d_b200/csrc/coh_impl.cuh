@@ -13,6 +13,7 @@
 //                    muy*r2c(Viscxy) + CS^2*r2c(Px) = r2c(NLx + (mux*Viscxx +
 //                    muy*Viscxy) + CS^2*Px), all masked by the same 2/3 rule.
 //   k_col_fwd_simple y-forward, dealiasing, sign, stepper update.
+#pragma once
 #include "models.h"
 
 namespace tara {
@@ -167,6 +168,10 @@ int coh_rhs(const Grid<T>& g, CohWork<T>& w, const CohParamsT<T>& p, Cx<T>* cons
   for (int q = 0; q < 8; q++) ci.job[q] = ColInvJob<T>{in[src[q]], w.H[q], mul[q]};
   run_col_inv(ci, 8, st);
 
+  if ((size_t)7 * (g.Nx / 2) * sizeof(Cx<T>) > 227 * 1024) {
+    set_error("hydro row pass does not fit in shared memory at this Nx and precision");
+    return TARA_EUNSUPPORTED;
+  }
   RowCohArgs<T> ra{};
   ra.tb = g.tb;
   for (int q = 0; q < 8; q++) ra.H[q] = w.H[q];
@@ -184,10 +189,5 @@ int coh_rhs(const Grid<T>& g, CohWork<T>& w, const CohParamsT<T>& p, Cx<T>* cons
   TARA_CUDA_TRY(cudaGetLastError());
   return TARA_OK;
 }
-
-template int coh_rhs<double>(const Grid<double>&, CohWork<double>&, const CohParamsT<double>&,
-                             Cx<double>* const[3], const StepArgs<double>&, cudaStream_t);
-template int coh_rhs<float>(const Grid<float>&, CohWork<float>&, const CohParamsT<float>&,
-                            Cx<float>* const[3], const StepArgs<float>&, cudaStream_t);
 
 }  // namespace tara
