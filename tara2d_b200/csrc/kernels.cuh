@@ -218,6 +218,52 @@ inline void run_col_fwd_simple(const ColFwdSimpleArgs<T>& a, int nf, cudaStream_
   TARA_DISPATCH_LEN(a.tb.Ny, col_fwd_simple_dispatch, a, nf, st)
 }
 
+// ------------------------------------------------------------ y round trip
+// dst = y-inverse( mul(ky) * y-forward(src) ): the y-derivative of an
+// x-transformed field, returned as a half-real field.
+template <class T> struct ColRtArgs {
+  Tables<T> tb;
+  const Cx<T>* src;
+  Cx<T>* dst;
+  int mul;
+};
+template <class T, int L, int CB, int P>
+__global__ void __launch_bounds__(CB * L / P) k_col_rt(const ColRtArgs<T> a) {
+  using F = FFTB<L, CB, P>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+  const int c0 = blockIdx.x * CB;
+  const int Nh = a.tb.Nh, ld = a.tb.ld;
+  const T* ky = a.tb.ky;
+  Cx<T> v[P];
+  fft_run<F, -1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
+    const int c = c0 + t;
+    if (c >= Nh) return cx<T>(0, 0);
+    return ldg(a.src + (size_t)i * ld + c);
+  }, SyncBlock{});
+  __syncthreads();
+  fft_emit<F>(threadIdx.x, v, [&](int t, int j, Cx<T> x) { sm[j * CB + t] = apply_ymul(a.mul, __ldg(ky + j), x); });
+  __syncthreads();
+  fft_run<F, +1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) { return sm[i * CB + t]; },
+                 SyncBlock{});
+  fft_emit<F>(threadIdx.x, v, [&](int t, int i, Cx<T> x) {
+    const int c = c0 + t;
+    if (c < Nh) st(a.dst + (size_t)i * ld + c, x);
+  });
+}
+template <int L, class T>
+inline void col_rt_dispatch(const ColRtArgs<T>& a, cudaStream_t st) {
+  constexpr int CB = ColCfg<T, L>::CB, P = ColCfg<T, L>::P;
+  auto kern = k_col_rt<T, L, CB, P>;
+  const size_t smem = col_smem_bytes<T, L>();
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<(a.tb.Nh + CB - 1) / CB, CB * L / P, smem, st>>>(a);
+}
+template <class T>
+inline void run_col_rt(const ColRtArgs<T>& a, cudaStream_t st) {
+  TARA_DISPATCH_LEN(a.tb.Ny, col_rt_dispatch, a, st)
+}
+
 // rows per CTA for a row kernel with ntr threads per row
 inline int rows_per_cta(int ntr, int Ny, size_t smem_per_row) {
   int rb = 1;

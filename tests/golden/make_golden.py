@@ -41,6 +41,9 @@ def main():
     d = O.derive2coh(16, 16, coh_params(), *st)
     np.savez(os.path.join(HERE, "derive2coh_16.npz"), nk=st[0], ukx=st[1], uky=st[2], dn=d[0], dux=d[1], duy=d[2])
     sm = I.com_orszag_tang(16, 16, seed=7, amp=1e-2, kmin=2, kmax=5)
+    # compressive noise on every mode, so that d(rho)/dt is not rounding noise
+    sm = [a + 1e-3 * np.abs(a).max() * (rng.standard_normal(a.shape) + 1j * rng.standard_normal(a.shape))
+          for a in sm]
     dm = O.derive2com(16, 16, com_params(0), sm)
     np.savez(os.path.join(HERE, "derive2com_16.npz"), state=np.array(sm), rhs=np.array(dm))
 
