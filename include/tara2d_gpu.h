@@ -27,6 +27,7 @@
  */
 #ifndef TARA2D_GPU_H
 #define TARA2D_GPU_H
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -94,6 +95,20 @@ int tara_synchronize(tara_session* s);
 int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms);
 /* Kernel launches one step of the given stepper issues. */
 int tara_launches_per_step(const tara_session* s, int stepper);
+/* Advance nsteps with a CUDA event recorded before every kernel; returns, per
+ * kernel kind (index 0..TARA_NUM_KERNEL_KINDS-1, see tara_kernel_name), the
+ * summed device time in ms and the number of launches, plus the total. */
+#define TARA_NUM_KERNEL_KINDS 10
+int tara_profile_steps(tara_session* s, int stepper, int nsteps, double* kernel_ms, int* kernel_launches,
+                       float* total_ms);
+const char* tara_kernel_name(int kind);
+/* Page-lock (pin) a host range for fast host<->device copies, and undo it. */
+int tara_host_register(void* p, size_t bytes);
+int tara_host_unregister(void* p);
+/* PCI bus id ("0000:xx:yy.z") of the current CUDA device. */
+int tara_device_pci_bus_id(char* out, int len);
+/* Select the CUDA device of the calling thread for later tara_open calls. */
+int tara_set_device(int dev);
 /* Sticky error of the session (first failure), TARA_OK if none. */
 int tara_status(const tara_session* s);
 /* Description of the last error of the calling thread ("" if none). */

@@ -26,6 +26,7 @@ FP64, FP32 = 0, 1
 STEP_AB2, STEP_RK4, STEP_EULER = 0, 1, 2
 LEGACY_REFERENCE, LEGACY_CORRECT = 0, 1
 SUPPORTED_N = (16, 32, 64, 128, 256, 384, 512, 1024, 2048, 4096)
+NUM_KERNEL_KINDS = 10
 NFIELDS = {MODEL_COH: 3, MODEL_COM: 6, MODEL_CSH: 1, MODEL_CSS: 1}
 PI = 3.14159265358979323846
 
@@ -78,6 +79,13 @@ def lib():
         L.tara_derive2coh.argtypes = [C.POINTER(Params), I, I, P, P, P, P, P, P]
         L.tara_derive2com.argtypes = [C.POINTER(Params), I, I, PP, PP]
         L.tara_set_legacy_mode.argtypes = [I]
+        L.tara_profile_steps.argtypes = [P, I, I, C.POINTER(C.c_double), C.POINTER(C.c_int), C.POINTER(C.c_float)]
+        L.tara_kernel_name.restype = C.c_char_p
+        L.tara_kernel_name.argtypes = [I]
+        L.tara_host_register.argtypes = [P, C.c_size_t]
+        L.tara_host_unregister.argtypes = [P]
+        L.tara_device_pci_bus_id.argtypes = [C.c_char_p, I]
+        L.tara_set_device.argtypes = [I]
         _lib = L
     return _lib
 
@@ -145,6 +153,11 @@ class Session:
         check(lib().tara_get_state(self._h, _ptrs(out)), "tara_get_state")
         return out
 
+    def get_state_into(self, out) -> None:
+        """Copy the state into caller-owned (e.g. pinned) (Ny, Nh) complex128 arrays."""
+        assert len(out) == self.nf and all(a.flags.c_contiguous and a.dtype == np.complex128 for a in out)
+        check(lib().tara_get_state(self._h, _ptrs(out)), "tara_get_state")
+
     def set_history(self, fields) -> None:
         a = self._fields_in(fields)
         check(lib().tara_set_history(self._h, _ptrs(a)), "tara_set_history")
@@ -172,6 +185,19 @@ class Session:
 
     def launches_per_step(self, stepper: int) -> int:
         return lib().tara_launches_per_step(self._h, stepper)
+
+    def profile_steps(self, stepper: int, nsteps: int):
+        """Per-kernel device time: {name: (total_ms, launches)} and the total ms."""
+        n = NUM_KERNEL_KINDS
+        ms = (C.c_double * n)()
+        cnt = (C.c_int * n)()
+        tot = C.c_float()
+        check(lib().tara_profile_steps(self._h, stepper, nsteps, ms, cnt, C.byref(tot)), "tara_profile_steps")
+        out = {}
+        for k in range(n):
+            if cnt[k]:
+                out[lib().tara_kernel_name(k).decode()] = (ms[k], cnt[k])
+        return out, tot.value
 
     @property
     def status(self) -> int:
@@ -221,3 +247,22 @@ def legacy_call(name: str, Nx: int, Ny: int, pi: float, time: float, arrays) -> 
 
 def set_legacy_mode(mode: int) -> None:
     check(lib().tara_set_legacy_mode(mode), "tara_set_legacy_mode")
+
+
+def pin(a: np.ndarray) -> None:
+    """Page-lock a numpy array's memory (fast DMA for set_state/get_state)."""
+    check(lib().tara_host_register(C.c_void_p(a.ctypes.data), a.nbytes), "tara_host_register")
+
+
+def unpin(a: np.ndarray) -> None:
+    check(lib().tara_host_unregister(C.c_void_p(a.ctypes.data)), "tara_host_unregister")
+
+
+def set_device(dev: int) -> None:
+    check(lib().tara_set_device(int(dev)), "tara_set_device")
+
+
+def device_pci_bus_id() -> str:
+    buf = C.create_string_buffer(64)
+    check(lib().tara_device_pci_bus_id(buf, 64), "tara_device_pci_bus_id")
+    return buf.value.decode()

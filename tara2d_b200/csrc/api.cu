@@ -90,6 +90,7 @@ struct tara_session {
   cudaStream_t st = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int status = TARA_OK;
+  Prof prof;
   virtual ~tara_session() {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -120,7 +121,7 @@ namespace {
 template <class T>
 struct SessionT : tara_session {
   Grid<T> g;
-  FieldPool<T> u, dold, acc, us, tmp;
+  FieldPool<T> u, unew, dold, acc, us, us2, tmp;
   FieldPool<double> stage;  // FP32 sessions: FP64 staging of host transfers
   CohWork<T> cw;
   ComWork<T> mw;
@@ -131,16 +132,20 @@ struct SessionT : tara_session {
 
   ~SessionT() override {
     if (st) cudaStreamSynchronize(st);
-    g.release(); u.release(); dold.release(); acc.release(); us.release(); tmp.release();
+    g.release(); u.release(); unew.release(); dold.release(); acc.release(); us.release(); us2.release();
+    tmp.release();
     stage.release(); cw.release(); mw.release(); vw.release();
   }
 
   int init() override {
     TARA_TRY(g.init(Nx, Ny, p.Lx, p.Ly, p.pi, st));
+    g.prof = &prof;
     TARA_TRY(u.alloc(g, nf, st));
     TARA_TRY(dold.alloc(g, nf, st));
     TARA_TRY(acc.alloc(g, nf, st));
     TARA_TRY(us.alloc(g, nf, st));
+    TARA_TRY(us2.alloc(g, nf, st));
+    TARA_TRY(unew.alloc(g, nf, st));
     TARA_TRY(tmp.alloc(g, nf, st));
     if (sizeof(T) != sizeof(double)) {
       // staging as complex128 [Ny][Nh] (host layout, no pitch)
@@ -168,6 +173,7 @@ struct SessionT : tara_session {
       TARA_CUDA_TRY(cudaStreamSynchronize(st));
       g.release();
       TARA_TRY(g.init(Nx, Ny, p.Lx, p.Ly, p.pi, st));
+      g.prof = &prof;
     }
     cohp.mux = (T)p.mux;
     cohp.muy = (T)p.muy;
@@ -243,6 +249,7 @@ struct SessionT : tara_session {
     for (int f = 0; f < nf; f++) {
       s.out[f] = tmp[f];
       s.u[f] = u[f];
+      s.unew[f] = unew[f];
       s.dold[f] = dold[f];
       s.acc[f] = acc[f];
       s.us[f] = us[f];
@@ -257,30 +264,39 @@ struct SessionT : tara_session {
     for (int f = 0; f < nf; f++) TARA_TRY(d2h(tmp[f], out[f]));
     return TARA_OK;
   }
+  // One step reads the state from `u` and writes the new state to `unew`
+  // (the RHS of one field reads other fields of its input state, so no
+  // kernel may update a state it also reads); the two are swapped after the
+  // step.  RK4 stage inputs alternate between us and us2 for the same reason.
   int step(int stepper, int n) override {
-    Cx<T>* in_u[6];
-    Cx<T>* in_s[6];
-    for (int f = 0; f < nf; f++) { in_u[f] = u[f]; in_s[f] = us[f]; }
+    if (stepper != TARA_STEP_AB2 && stepper != TARA_STEP_EULER && stepper != TARA_STEP_RK4) {
+      set_error("unknown stepper");
+      return TARA_EINVAL;
+    }
     for (int t = 0; t < n; t++) {
-      if (stepper == TARA_STEP_AB2) {
-        TARA_TRY(rhs(in_u, base_args(STEP_AB2)));
-      } else if (stepper == TARA_STEP_EULER) {
-        TARA_TRY(rhs(in_u, base_args(STEP_EULER)));
-      } else if (stepper == TARA_STEP_RK4) {
+      Cx<T>* in_u[6];
+      for (int f = 0; f < nf; f++) in_u[f] = u[f];
+      if (stepper == TARA_STEP_AB2 || stepper == TARA_STEP_EULER) {
+        TARA_TRY(rhs(in_u, base_args(stepper == TARA_STEP_AB2 ? STEP_AB2 : STEP_EULER)));
+      } else {
         // classical RK4; weights and stage offsets as in the oracle:
-        // acc = u + (w dt/6) k1 ; us = u + (c dt) k ; u = acc + (dt/6) k4
+        // acc = u + (w dt/6) k1 ; us = u + (c dt) k ; u_new = acc + (dt/6) k4
         const double w[4] = {1.0, 2.0, 2.0, 1.0}, c[3] = {0.5, 0.5, 1.0};
+        FieldPool<T>* ping[2] = {&us, &us2};
         for (int s = 0; s < 4; s++) {
           StepArgs<T> a = base_args(STEP_RK4);
           a.stage = s;
           a.wa = (T)(w[s] * p.dt / 6.0);
           a.cs = s < 3 ? (T)(c[s] * p.dt) : (T)0;
-          TARA_TRY(rhs(s == 0 ? in_u : in_s, a));
+          Cx<T>* in[6];
+          for (int f = 0; f < nf; f++) {
+            in[f] = s == 0 ? u[f] : (*ping[(s - 1) & 1])[f];
+            a.us[f] = (*ping[s & 1])[f];
+          }
+          TARA_TRY(rhs(in, a));
         }
-      } else {
-        set_error("unknown stepper");
-        return TARA_EINVAL;
       }
+      std::swap(u, unew);
     }
     return TARA_OK;
   }
@@ -437,6 +453,83 @@ int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms) {
   cudaEventElapsedTime(ms, s->ev0, s->ev1);
   return TARA_OK;
 }
+int tara_profile_steps(tara_session* s, int stepper, int nsteps, double* kernel_ms, int* kernel_launches,
+                       float* total_ms) {
+  if (!s || !kernel_ms || !kernel_launches || nsteps < 0) return TARA_EINVAL;
+  for (int k = 0; k < TARA_NUM_KERNEL_KINDS; k++) { kernel_ms[k] = 0; kernel_launches[k] = 0; }
+  if (cudaStreamSynchronize(s->st) != cudaSuccess) return s->fail_if(TARA_ECUDA);
+  Prof& pr = s->prof;
+  pr.cap = nsteps * (s->launches(stepper) * 2 + 8) + 8;
+  pr.ev = new cudaEvent_t[pr.cap];
+  pr.kind = new int[pr.cap];
+  int made = 0, r = TARA_OK;
+  for (; made < pr.cap; made++)
+    if (cudaEventCreate(&pr.ev[made]) != cudaSuccess) { r = TARA_ECUDA; break; }
+  if (r == TARA_OK) {
+    pr.n = 0;
+    pr.on = 1;
+    cudaEventRecord(s->ev0, s->st);
+    r = s->step(stepper, nsteps);
+    cudaEventRecord(s->ev1, s->st);
+    pr.on = 0;
+    if (r == TARA_OK && cudaEventSynchronize(s->ev1) != cudaSuccess) r = TARA_ECUDA;
+    if (r == TARA_OK) {
+      if (total_ms) cudaEventElapsedTime(total_ms, s->ev0, s->ev1);
+      for (int i = 0; i + 1 < pr.n; i++) {
+        const int k = pr.kind[i];
+        if (k == KK_END) continue;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, pr.ev[i], pr.ev[i + 1]);
+        kernel_ms[k] += ms;
+        kernel_launches[k] += 1;
+      }
+    }
+  }
+  for (int i = 0; i < made; i++) cudaEventDestroy(pr.ev[i]);
+  delete[] pr.ev;
+  delete[] pr.kind;
+  pr.ev = nullptr;
+  pr.kind = nullptr;
+  pr.cap = pr.n = 0;
+  if (r != TARA_OK) set_error("profiling run failed");
+  return s->fail_if(r);
+}
+const char* tara_kernel_name(int kind) { return kernel_kind_name(kind); }
+
+int tara_host_register(void* p, size_t bytes) {
+  cudaError_t e = cudaHostRegister(p, bytes, cudaHostRegisterDefault);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaHostRegister: ") + cudaGetErrorString(e));
+    return TARA_ECUDA;
+  }
+  return TARA_OK;
+}
+int tara_host_unregister(void* p) {
+  cudaError_t e = cudaHostUnregister(p);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaHostUnregister: ") + cudaGetErrorString(e));
+    return TARA_ECUDA;
+  }
+  return TARA_OK;
+}
+int tara_set_device(int dev) {
+  cudaError_t e = cudaSetDevice(dev);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return TARA_ECUDA;
+  }
+  return TARA_OK;
+}
+int tara_device_pci_bus_id(char* out, int len) {
+  int dev = 0;
+  if (!out || len < 13) return TARA_EINVAL;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetPCIBusId(out, len, dev) != cudaSuccess) {
+    set_error("cudaDeviceGetPCIBusId failed");
+    return TARA_ECUDA;
+  }
+  return TARA_OK;
+}
+
 int tara_launches_per_step(const tara_session* s, int stepper) { return s ? s->launches(stepper) : 0; }
 int tara_status(const tara_session* s) { return s ? s->status : TARA_EINVAL; }
 

@@ -166,6 +166,7 @@ int coh_rhs(const Grid<T>& g, CohWork<T>& w, const CohParamsT<T>& p, Cx<T>* cons
   const int src[8] = {0, 0, 1, 1, 1, 2, 2, 2};
   const int mul[8] = {MUL_ONE, MUL_IKY, MUL_ONE, MUL_IKY, MUL_KY2, MUL_ONE, MUL_IKY, MUL_KY2};
   for (int q = 0; q < 8; q++) ci.job[q] = ColInvJob<T>{in[src[q]], w.H[q], mul[q]};
+  prof_mark(g.prof, st, KK_COL_INV);
   run_col_inv(ci, 8, st);
 
   if ((size_t)7 * (g.Nx / 2) * sizeof(Cx<T>) > 227 * 1024) {
@@ -179,13 +180,16 @@ int coh_rhs(const Grid<T>& g, CohWork<T>& w, const CohParamsT<T>& p, Cx<T>* cons
   ra.mux = p.mux;
   ra.muy = p.muy;
   ra.cs2 = p.cs2;
+  prof_mark(g.prof, st, KK_ROW_COH);
   TARA_DISPATCH_LEN(g.Nx, launch_row_coh, ra, g.Ny, st)
 
   ColFwdSimpleArgs<T> cf{};
   cf.tb = g.tb;
   for (int q = 0; q < 3; q++) { cf.X[q] = w.X[q]; cf.sign[q] = (T)-1; }
   cf.step = step;
+  prof_mark(g.prof, st, KK_COL_FWD_SIMPLE);
   run_col_fwd_simple(cf, 3, st);
+  prof_mark(g.prof, st, KK_END);
   TARA_CUDA_TRY(cudaGetLastError());
   return TARA_OK;
 }

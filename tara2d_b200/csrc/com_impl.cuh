@@ -356,6 +356,7 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   for (int q = 0; q < 6; q++) ci.job[q] = ColInvJob<T>{in[q], w.H[q], MUL_ONE};
   int nj = 6;
   if (p.fix_curlB) ci.job[nj++] = ColInvJob<T>{in[4], w.H[HIKYBX], MUL_IKY};
+  prof_mark(g.prof, st, KK_COL_INV);
   run_col_inv(ci, nj, st);
 
   RowCom1Args<T> r1{};
@@ -368,6 +369,7 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   r1.dx = (T)(g.Lx / g.Nx);
   r1.dy = (T)(g.Ly / g.Ny);
   r1.forcing = forcing;
+  prof_mark(g.prof, st, KK_ROW_COM1);
   TARA_DISPATCH_LEN(g.Nx, launch_row_com1, r1, g.Ny, st)
 
   ColRtArgs<T> rt{};
@@ -375,6 +377,7 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   rt.src = w.X[XUY];
   rt.dst = w.H[HDUY];
   rt.mul = MUL_IKY;
+  prof_mark(g.prof, st, KK_COL_RT);
   run_col_rt(rt, st);
 
   RowCom2Args<T> r2{};
@@ -390,6 +393,7 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   r2.eta = p.eta;
   r2.inv_nx = (T)(1.0 / g.Nx);
   r2.fix_curlB = p.fix_curlB;
+  prof_mark(g.prof, st, KK_ROW_COM2);
   TARA_DISPATCH_LEN(g.Nx, launch_row_com2, r2, g.Ny, st)
 
   ColFwdComArgs<T> cf{};
@@ -400,7 +404,9 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   cf.eta = p.eta;
   cf.forcing = forcing;
   cf.step = step;
+  prof_mark(g.prof, st, KK_COL_FWD_COM);
   TARA_DISPATCH_LEN(g.Ny, col_fwd_com_dispatch, cf, st)
+  prof_mark(g.prof, st, KK_END);
   TARA_CUDA_TRY(cudaGetLastError());
   return TARA_OK;
 }

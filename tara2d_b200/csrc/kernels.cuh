@@ -90,10 +90,11 @@ template <class T> struct StepArgs {
   T wa;        // RK4: weight*dt/6 of this stage
   T cs;        // RK4: c*dt of the next stage input
   Cx<T>* out[6];  // STEP_RHS: derivative output
-  Cx<T>* u[6];    // state (AB2/Euler: updated in place; RK4: base state)
-  Cx<T>* dold[6]; // AB2 history, replaced by the new derivative
+  Cx<T>* u[6];    // base state (read only)
+  Cx<T>* unew[6]; // new state (AB2, Euler, last RK4 stage); never aliases u or the RHS input
+  Cx<T>* dold[6]; // AB2 history, replaced by the new derivative (same element, same thread)
   Cx<T>* acc[6];  // RK4 accumulator
-  Cx<T>* us[6];   // RK4 next stage input
+  Cx<T>* us[6];   // RK4 next stage input; never aliases the current stage input
 };
 
 // d = derivative of field f at element idx.  Operation order follows
@@ -108,13 +109,13 @@ __device__ __forceinline__ void step_apply(const StepArgs<T>& s, int f, size_t i
       Cx<T> old = ld(s.dold[f] + idx);
       Cx<T> u = ld(s.u[f] + idx);
       Cx<T> inc = rmul((T)1.5, d) - rmul((T)0.5, old);
-      st(s.u[f] + idx, u + rmul(s.dt, inc));
+      st(s.unew[f] + idx, u + rmul(s.dt, inc));
       st(s.dold[f] + idx, d);
       break;
     }
     case STEP_EULER: {
       Cx<T> u = ld(s.u[f] + idx);
-      st(s.u[f] + idx, u + rmul(s.dt, d));
+      st(s.unew[f] + idx, u + rmul(s.dt, d));
       st(s.dold[f] + idx, d);
       break;
     }
@@ -130,7 +131,7 @@ __device__ __forceinline__ void step_apply(const StepArgs<T>& s, int f, size_t i
         st(s.us[f] + idx, u + rmul(s.cs, d));
       } else {
         Cx<T> a = ld(s.acc[f] + idx);
-        st(s.u[f] + idx, a + rmul(s.wa, d));
+        st(s.unew[f] + idx, a + rmul(s.wa, d));
       }
       break;
     }

@@ -5,6 +5,7 @@
 #include <string>
 #include <vector>
 #include "spectral.cuh"
+#include "prof.h"
 #include "../../include/tara2d_gpu.h"
 
 namespace tara {
@@ -43,6 +44,7 @@ struct Grid {
   int Nx = 0, Ny = 0, Nh = 0, ld = 0;
   double Lx = 0, Ly = 0, pi = 0;
   Tables<T> tb{};
+  Prof* prof = nullptr;  // per-kernel timing (owned by the session)
   void* dmem = nullptr;  // one allocation for all tables
   size_t field_elems() const { return (size_t)Ny * ld; }
   size_t field_bytes() const { return field_elems() * sizeof(Cx<T>); }
