@@ -211,7 +211,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=30)
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=1024, help="grid size (profiling runs only; the metric is at 1024)")
     args = ap.parse_args()
+    global N
+    N = args.grid
     if args.impl == "reference":
         return run_reference(args)
 

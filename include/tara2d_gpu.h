@@ -98,7 +98,7 @@ int tara_launches_per_step(const tara_session* s, int stepper);
 /* Advance nsteps with a CUDA event recorded before every kernel; returns, per
  * kernel kind (index 0..TARA_NUM_KERNEL_KINDS-1, see tara_kernel_name), the
  * summed device time in ms and the number of launches, plus the total. */
-#define TARA_NUM_KERNEL_KINDS 10
+#define TARA_NUM_KERNEL_KINDS 11
 int tara_profile_steps(tara_session* s, int stepper, int nsteps, double* kernel_ms, int* kernel_launches,
                        float* total_ms);
 const char* tara_kernel_name(int kind);

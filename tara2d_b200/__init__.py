@@ -26,7 +26,7 @@ FP64, FP32 = 0, 1
 STEP_AB2, STEP_RK4, STEP_EULER = 0, 1, 2
 LEGACY_REFERENCE, LEGACY_CORRECT = 0, 1
 SUPPORTED_N = (16, 32, 64, 128, 256, 384, 512, 1024, 2048, 4096)
-NUM_KERNEL_KINDS = 10
+NUM_KERNEL_KINDS = 11
 NFIELDS = {MODEL_COH: 3, MODEL_COM: 6, MODEL_CSH: 1, MODEL_CSS: 1}
 PI = 3.14159265358979323846
 

@@ -26,22 +26,22 @@ template <class T> struct RowCohArgs {
   int rb;
 };
 
+// One group per transform.  Phase 1: eleven c2r in eleven groups (each
+// group's output array is its exchange buffer).  Phase 2: the products, in
+// place.  Phase 3: three r2c, exchange buffers in the freed arrays 3..5.
 template <class T, int M, int P>
-__global__ void __launch_bounds__(128) k_row_coh(const RowCohArgs<T> a) {
+__global__ void __launch_bounds__(TARA_ROW_LB(11 * (M / P))) k_row_coh(const RowCohArgs<T> a) {
   using RF = RowFFT<M, P>;
-  constexpr int NTR = M / P;
+  constexpr int NTR = M / P, G = 11, ARR = RF::SMEM_ELEMS;
   extern __shared__ __align__(16) unsigned char smraw[];
-  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
-  const int r = threadIdx.x / NTR, lane = threadIdx.x % NTR;
-  const int y = blockIdx.x * a.rb + r;
+  const RowThread<NTR, G> th;
+  const auto sync = th.sync();
   const Tables<T>& tb = a.tb;
-  Cx<T>* xs = sm + (size_t)r * 7 * M;
-  Cx<T>* rn = xs + M;       // real fields stored as pairs (x[2m], x[2m+1])
-  Cx<T>* rux = xs + 2 * M;
-  Cx<T>* ruy = xs + 3 * M;
-  Cx<T>* fn = xs + 4 * M;
-  Cx<T>* fx = xs + 5 * M;
-  Cx<T>* fy = xs + 6 * M;
+  Cx<T>* base = reinterpret_cast<Cx<T>*>(smraw) + (size_t)th.row * G * ARR;
+  // 0 n, 1 ux, 2 uy, 3 dn/dx, 4 dn/dy, 5 dux/dx, 6 dux/dy, 7 duy/dx, 8 duy/dy,
+  // 9 mux d2ux/dx2 + muy d2ux/dy2, 10 mux d2uy/dx2 + muy d2uy/dy2   (pairs x[2m], x[2m+1])
+  auto arr = [&](int q) { return base + q * ARR; };
+  const int y = blockIdx.x * a.rb + th.row;
   const size_t ro = (size_t)y * tb.ld;
   const Cx<T>* Hn = a.H[0] + ro;
   const Cx<T>* Hny = a.H[1] + ro;
@@ -54,94 +54,62 @@ __global__ void __launch_bounds__(128) k_row_coh(const RowCohArgs<T> a) {
   const T* kx = tb.kx;
   const T mux = a.mux, muy = a.muy, cs2 = a.cs2;
   Cx<T> v[P];
-
-  auto store = [&](Cx<T>* dst) {
-    fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
+  // phase 1: c2r along x                          (src/derive2coh.f95:92-151)
+  {
+    const int g = th.g;
+    Cx<T>* dst = arr(g);
+    row_c2r<RF>(dst, th.lane, v, tb, [&](int k) -> Cx<T> {
+      const T k1 = __ldg(kx + k);
+      switch (g) {
+        case 0: return ldg(Hn + k);
+        case 1: return ldg(Hux + k);
+        case 2: return ldg(Huy + k);
+        case 3: return ikmul(k1, ldg(Hn + k));
+        case 4: return ldg(Hny + k);
+        case 5: return ikmul(k1, ldg(Hux + k));
+        case 6: return ldg(Huxy + k);
+        case 7: return ikmul(k1, ldg(Huy + k));
+        case 8: return ldg(Huyy + k);
+        case 9: return rmul(mux, rmul(k1 * k1, ldg(Hux + k))) + rmul(muy, ldg(Huxyy + k));
+        default: return rmul(mux, rmul(k1 * k1, ldg(Huy + k))) + rmul(muy, ldg(Huyyy + k));
+      }
+    }, sync);
+    sync();
+    fft_emit<RF>(th.lane, v, [&](int, int n, Cx<T> z) {
       dst[n] = cx<T>(normalise(z.x, tb), normalise(z.y, tb));
     });
-  };
-  // n, ux, uy                                   (src/derive2coh.f95:92-99)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(Hn + k); });
-  store(rn);
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(Hux + k); });
-  store(rux);
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(Huy + k); });
-  store(ruy);
-
-  // dn/dx: NLn = ux*dn/dx + ..., Px = dn/dx / n   (:158, :162)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ikmul(__ldg(kx + k), ldg(Hn + k)); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-    const T d0 = normalise(z.x, tb), d1 = normalise(z.y, tb);
-    const Cx<T> N = rn[n], U = rux[n];
-    fn[n] = cx<T>(U.x * d0, U.y * d1);
-    fx[n] = cx<T>(cs2 * (d0 / N.x), cs2 * (d1 / N.y));
-  });
-  // dn/dy                                        (:159, :162)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(Hny + k); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-    const T d0 = normalise(z.x, tb), d1 = normalise(z.y, tb);
-    const Cx<T> N = rn[n], V = ruy[n], F = fn[n];
-    fn[n] = cx<T>(F.x + V.x * d0, F.y + V.y * d1);
-    fy[n] = cx<T>(cs2 * (d0 / N.x), cs2 * (d1 / N.y));
-  });
-  // dux/dx: NLn += n*dux/dx, NLx = ux*dux/dx     (:162, :164)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ikmul(__ldg(kx + k), ldg(Hux + k)); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-    const T d0 = normalise(z.x, tb), d1 = normalise(z.y, tb);
-    const Cx<T> N = rn[n], U = rux[n], F = fn[n], G = fx[n];
-    fn[n] = cx<T>(F.x + N.x * d0, F.y + N.y * d1);
-    fx[n] = cx<T>(G.x + U.x * d0, G.y + U.y * d1);
-  });
-  // duy/dy: NLn += n*duy/dy, NLy = uy*duy/dy     (:162, :165)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(Huyy + k); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-    const T d0 = normalise(z.x, tb), d1 = normalise(z.y, tb);
-    const Cx<T> N = rn[n], V = ruy[n], F = fn[n], G = fy[n];
-    fn[n] = cx<T>(F.x + N.x * d0, F.y + N.y * d1);
-    fy[n] = cx<T>(G.x + V.x * d0, G.y + V.y * d1);
-  });
-  // dux/dy: NLx += uy*dux/dy                     (:164)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(Huxy + k); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-    const T d0 = normalise(z.x, tb), d1 = normalise(z.y, tb);
-    const Cx<T> V = ruy[n], G = fx[n];
-    fx[n] = cx<T>(G.x + V.x * d0, G.y + V.y * d1);
-  });
-  // duy/dx: NLy += ux*duy/dx                     (:165)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ikmul(__ldg(kx + k), ldg(Huy + k)); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-    const T d0 = normalise(z.x, tb), d1 = normalise(z.y, tb);
-    const Cx<T> U = rux[n], G = fy[n];
-    fy[n] = cx<T>(G.x + U.x * d0, G.y + U.y * d1);
-  });
-  // viscous x: (mux*d2ux/dx2 + muy*d2ux/dy2)/n   (:153-154, :251)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) {
-    const T k2 = __ldg(kx + k) * __ldg(kx + k);
-    return rmul(mux, rmul(k2, ldg(Hux + k))) + rmul(muy, ldg(Huxyy + k));
-  });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-    const T d0 = normalise(z.x, tb), d1 = normalise(z.y, tb);
-    const Cx<T> N = rn[n], G = fx[n];
-    fx[n] = cx<T>(G.x + d0 / N.x, G.y + d1 / N.y);
-  });
-  // viscous y                                    (:155-156, :252)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) {
-    const T k2 = __ldg(kx + k) * __ldg(kx + k);
-    return rmul(mux, rmul(k2, ldg(Huy + k))) + rmul(muy, ldg(Huyyy + k));
-  });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-    const T d0 = normalise(z.x, tb), d1 = normalise(z.y, tb);
-    const Cx<T> N = rn[n], G = fy[n];
-    fy[n] = cx<T>(G.x + d0 / N.x, G.y + d1 / N.y);
-  });
+  }
   __syncthreads();
-  // three r2c along x                            (:172-197 merged)
-  Cx<T>* Xn = a.X[0] + ro;
-  Cx<T>* Xx = a.X[1] + ro;
-  Cx<T>* Xy = a.X[2] + ro;
-  row_r2c<RF>(xs, lane, NTR, v, tb, [&](int n) { return fn[n]; }, [&](int k, Cx<T> X) { st(Xn + k, X); });
-  row_r2c<RF>(xs, lane, NTR, v, tb, [&](int n) { return fx[n]; }, [&](int k, Cx<T> X) { st(Xx + k, X); });
-  row_r2c<RF>(xs, lane, NTR, v, tb, [&](int n) { return fy[n]; }, [&](int k, Cx<T> X) { st(Xy + k, X); });
+  // phase 2: products                              (:153-165)
+  //   NLn = ux dn/dx + uy dn/dy + n (dux/dx + duy/dy)
+  //   Fx  = (ux dux/dx + uy dux/dy) + visc_x/n + CS^2 (dn/dx)/n   (+ same for y)
+  for (int m = th.g * NTR + th.lane; m < M; m += G * NTR) {
+    T q[11][2];
+#pragma unroll
+    for (int f = 0; f < 11; f++) {
+      const Cx<T> z = arr(f)[m];
+      q[f][0] = z.x;
+      q[f][1] = z.y;
+    }
+    T o[3][2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const T n = q[0][h], ux = q[1][h], uy = q[2][h];
+      o[0][h] = ux * q[3][h] + uy * q[4][h] + n * (q[5][h] + q[8][h]);
+      o[1][h] = (ux * q[5][h] + uy * q[6][h]) + q[9][h] / n + cs2 * (q[3][h] / n);
+      o[2][h] = (ux * q[7][h] + uy * q[8][h]) + q[10][h] / n + cs2 * (q[4][h] / n);
+    }
+#pragma unroll
+    for (int f = 0; f < 3; f++) arr(f)[m] = cx<T>(o[f][0], o[f][1]);
+  }
+  __syncthreads();
+  // phase 3: three r2c along x                     (:172-197, merged by linearity)
+  if (th.g < 3) {
+    const int g = th.g;
+    row_r2c_begin<RF>(th.lane, v, tb, [&](int n) { return arr(g)[n]; });
+    Cx<T>* xo = a.X[g] + ro;
+    row_r2c_finish<RF>(arr(3 + g), th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
+  }
 }
 
 template <int Nx, class T>
@@ -150,12 +118,13 @@ static void launch_row_coh(const RowCohArgs<T>& a0, int Ny, cudaStream_t st) {
   constexpr int P = RowCfg<M>::P;
   constexpr int NTR = M / P;
   RowCohArgs<T> a = a0;
-  const size_t per_row = (size_t)7 * M * sizeof(Cx<T>);
-  a.rb = rows_per_cta(NTR, Ny, per_row);
+  const size_t per_row = (size_t)11 * RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<T>);
+  a.rb = 1;
+  while (a.rb * 2 * 11 * NTR <= 128 && Ny % (a.rb * 2) == 0 && (a.rb * 2) * per_row <= 110 * 1024) a.rb *= 2;
   auto kern = k_row_coh<T, M, P>;
   const size_t smem = per_row * a.rb;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<Ny / a.rb, NTR * a.rb, smem, st>>>(a);
+  kern<<<Ny / a.rb, 11 * NTR * a.rb, smem, st>>>(a);
 }
 
 template <class T>
@@ -169,7 +138,7 @@ int coh_rhs(const Grid<T>& g, CohWork<T>& w, const CohParamsT<T>& p, Cx<T>* cons
   prof_mark(g.prof, st, KK_COL_INV);
   run_col_inv(ci, 8, st);
 
-  if ((size_t)7 * (g.Nx / 2) * sizeof(Cx<T>) > 227 * 1024) {
+  if ((size_t)11 * (g.Nx / 2 + g.Nx / 32 + 1) * sizeof(Cx<T>) > 227 * 1024 || 11 * (g.Nx / 2) / 16 > 1024) {
     set_error("hydro row pass does not fit in shared memory at this Nx and precision");
     return TARA_EUNSUPPORTED;
   }

@@ -28,96 +28,140 @@ namespace tara {
 enum : int { XUX = 0, XUY, XMXX, XMXY, XMYY, XMAG, XEX, XEY, XEV, XFX, XFY };
 enum : int { HRHO = 0, HMX, HMY, HE, HBX, HBY, HDUY, HIKYBX };
 
+// Rows per CTA so that a CTA has at least ~128 threads, within the shared
+// memory budget and dividing Ny.
+inline int row_cta_rows(int threads_per_row, size_t smem_per_row, int Ny, int max_threads = 1024) {
+  int rb = 1;
+  while (rb * 2 * threads_per_row <= 128 && rb * 2 * threads_per_row <= max_threads && Ny % (rb * 2) == 0 &&
+         (rb * 2) * smem_per_row <= 110 * 1024)
+    rb *= 2;
+  return rb;
+}
+
+// ---------------------------------------------------------------- row pass 1
+// One group per transform: phase 1 runs the six c2r of a row in six groups
+// (each group's output array is also its exchange buffer), phase 2 forms the
+// velocity, phase 3 runs the eight r2c in eight groups; once every group has
+// gathered its inputs the eight field arrays become their exchange buffers.
 template <class T> struct RowCom1Args {
   Tables<T> tb;
   const Cx<T>* H[6];
   Cx<T>* X[11];
-  T cs2, A, kf, dx, dy;
-  int forcing, rb;
+  T cs2;
+  int rb;
 };
 
 template <class T, int M, int P>
-__global__ void __launch_bounds__(128) k_row_com1(const RowCom1Args<T> a) {
+__global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const RowCom1Args<T> a) {
   using RF = RowFFT<M, P>;
-  constexpr int NTR = M / P;
+  constexpr int NTR = M / P, G = 8, ARR = RF::SMEM_ELEMS;
   extern __shared__ __align__(16) unsigned char smraw[];
-  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
-  const int r = threadIdx.x / NTR, lane = threadIdx.x % NTR;
-  const int y = blockIdx.x * a.rb + r;
+  const RowThread<NTR, G> th;
+  const auto sync = th.sync();
   const Tables<T>& tb = a.tb;
-  Cx<T>* xs = sm + (size_t)r * 9 * M;
-  Cx<T>* f[8];  // rho, rho ux, rho uy, E, Bx, By, ux, uy (pairs)
+  Cx<T>* base = reinterpret_cast<Cx<T>*>(smraw) + (size_t)th.row * G * ARR;
+  Cx<T>* f[8];  // rho, rho ux, rho uy, E, Bx, By, ux, uy (pairs x[2m], x[2m+1])
 #pragma unroll
-  for (int q = 0; q < 8; q++) f[q] = xs + (q + 1) * M;
+  for (int q = 0; q < 8; q++) f[q] = base + q * ARR;
+  const int y = blockIdx.x * a.rb + th.row;
   const size_t ro = (size_t)y * tb.ld;
   Cx<T> v[P];
-  // six c2r along x, normalised                (src/derive2com.f95:70-102)
-#pragma unroll 1
-  for (int q = 0; q < 6; q++) {
-    const Cx<T>* h = a.H[q] + ro;
-    row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(h + k); });
-    Cx<T>* dst = f[q];
-    fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
+  // phase 1: six c2r along x, normalised         (src/derive2com.f95:70-102)
+  if (th.g < 6) {
+    const Cx<T>* h = a.H[th.g] + ro;
+    Cx<T>* dst = f[th.g];
+    row_c2r<RF>(dst, th.lane, v, tb, [&](int k) { return ldg(h + k); }, sync);
+    sync();
+    fft_emit<RF>(th.lane, v, [&](int, int n, Cx<T> z) {
       dst[n] = cx<T>(normalise(z.x, tb), normalise(z.y, tb));
     });
   }
-  // velocity                                    (:105-106)
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T>) {
+  __syncthreads();
+  // phase 2: velocity                            (:105-106)
+  for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
     const Cx<T> rho = f[0][n], mx = f[1][n], my = f[2][n];
     f[6][n] = cx<T>(mx.x / rho.x, mx.y / rho.y);
     f[7][n] = cx<T>(my.x / rho.x, my.y / rho.y);
-  });
-  __syncthreads();
-  const T cs2 = a.cs2;
-  // fluxes of one grid point                    (:193-213)
-  auto flux = [&](int which, int n, int half) -> T {
-    const T rho = half ? f[0][n].y : f[0][n].x;
-    const T mx = half ? f[1][n].y : f[1][n].x;
-    const T my = half ? f[2][n].y : f[2][n].x;
-    const T E = half ? f[3][n].y : f[3][n].x;
-    const T bx = half ? f[4][n].y : f[4][n].x;
-    const T by = half ? f[5][n].y : f[5][n].x;
-    const T ux = half ? f[6][n].y : f[6][n].x;
-    const T uy = half ? f[7][n].y : f[7][n].x;
-    const T B2 = bx * bx + by * by;
-    const T Pr = cs2 * rho;
-    switch (which) {
-      case XUX: return ux;
-      case XUY: return uy;
-      case XMXX: return mx * ux + Pr + B2 / (T)2 - bx * bx;
-      case XMXY: return mx * uy - bx * by;
-      case XMYY: return my * uy + Pr + B2 / (T)2 - by * by;
-      case XMAG: return uy * bx - by * ux;
-      case XEX: return (E + Pr + B2 / (T)2) * ux - ux * bx * bx - uy * bx * by;
-      case XEY: return (E + Pr + B2 / (T)2) * uy - ux * bx * by - uy * by * by;
-      default: return (T)0;
-    }
-  };
-  const int nout = a.forcing ? 11 : 8;
-#pragma unroll 1
-  for (int q = 0; q < nout; q++) {
-    if (q == XEV) continue;
-    Cx<T>* xo = a.X[q] + ro;
-    row_r2c<RF>(xs, lane, NTR, v, tb,
-                [&](int n) -> Cx<T> {
-                  if (q == XFX || q == XFY) {
-                    // Fx = -rho A sin(kf y_j), Fy = rho A sin(kf x_i) on the grid
-                    // x_i = (i-1) dx, y_j = (j-1) dy                      (:109-110)
-                    const Cx<T> rho = f[0][n];
-                    if (q == XFX) {
-                      const T s = sin(a.kf * ((T)y * a.dy));
-                      return cx<T>(-rho.x * a.A * s, -rho.y * a.A * s);
-                    }
-                    const T s0 = sin(a.kf * ((T)(2 * n) * a.dx));
-                    const T s1 = sin(a.kf * ((T)(2 * n + 1) * a.dx));
-                    return cx<T>(rho.x * a.A * s0, rho.y * a.A * s1);
-                  }
-                  return cx<T>(flux(q, n, 0), flux(q, n, 1));
-                },
-                [&](int k, Cx<T> X) { st(xo + k, X); });
   }
+  __syncthreads();
+  // phase 3: fluxes of output th.g at the stage-0 points, then r2c     (:193-213)
+  const T cs2 = a.cs2;
+  const int q = th.g;
+  row_r2c_begin<RF>(th.lane, v, tb, [&](int n) -> Cx<T> {
+    T o[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const T rho = h ? f[0][n].y : f[0][n].x;
+      const T mx = h ? f[1][n].y : f[1][n].x;
+      const T my = h ? f[2][n].y : f[2][n].x;
+      const T E = h ? f[3][n].y : f[3][n].x;
+      const T bx = h ? f[4][n].y : f[4][n].x;
+      const T by = h ? f[5][n].y : f[5][n].x;
+      const T ux = h ? f[6][n].y : f[6][n].x;
+      const T uy = h ? f[7][n].y : f[7][n].x;
+      const T B2 = bx * bx + by * by;
+      const T Pr = cs2 * rho;
+      T r;
+      switch (q) {
+        case XUX: r = ux; break;
+        case XUY: r = uy; break;
+        case XMXX: r = mx * ux + Pr + B2 / (T)2 - bx * bx; break;
+        case XMXY: r = mx * uy - bx * by; break;
+        case XMYY: r = my * uy + Pr + B2 / (T)2 - by * by; break;
+        case XMAG: r = uy * bx - by * ux; break;
+        case XEX: r = (E + Pr + B2 / (T)2) * ux - ux * bx * bx - uy * bx * by; break;
+        default: r = (E + Pr + B2 / (T)2) * uy - ux * bx * by - uy * by * by; break;  // XEY
+      }
+      o[h] = r;
+    }
+    return cx<T>(o[0], o[1]);
+  });
+  __syncthreads();  // every group has its inputs: the field arrays are free
+  Cx<T>* xo = a.X[q] + ro;
+  row_r2c_finish<RF>(f[q], th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
 }
 
+// Forcing (only when A != 0):  Fx = -rho A sin(kf y_j), Fy = rho A sin(kf x_i)
+// on the grid x_i = (i-1) dx, y_j = (j-1) dy                       (:109-110)
+template <class T> struct RowForceArgs {
+  Tables<T> tb;
+  const Cx<T>* Hrho;
+  Cx<T>* Xfx;
+  Cx<T>* Xfy;
+  T A, kf, dx, dy;
+  int rb;
+};
+template <class T, int M, int P>
+__global__ void __launch_bounds__(TARA_ROW_LB(2 * (M / P))) k_row_force(const RowForceArgs<T> a) {
+  using RF = RowFFT<M, P>;
+  constexpr int NTR = M / P, G = 2, ARR = RF::SMEM_ELEMS;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const RowThread<NTR, G> th;
+  const auto sync = th.sync();
+  const Tables<T>& tb = a.tb;
+  Cx<T>* rho = reinterpret_cast<Cx<T>*>(smraw) + (size_t)th.row * 3 * ARR;
+  Cx<T>* xs = rho + (1 + th.g) * ARR;
+  const int y = blockIdx.x * a.rb + th.row;
+  const size_t ro = (size_t)y * tb.ld;
+  Cx<T> v[P];
+  if (th.g == 0) {
+    row_c2r<RF>(xs, th.lane, v, tb, [&](int k) { return ldg(a.Hrho + ro + k); }, sync);
+    fft_emit<RF>(th.lane, v, [&](int, int n, Cx<T> z) { rho[n] = cx<T>(normalise(z.x, tb), normalise(z.y, tb)); });
+  }
+  __syncthreads();
+  const T sy = sin(a.kf * ((T)y * a.dy));
+  row_r2c_begin<RF>(th.lane, v, tb, [&](int n) -> Cx<T> {
+    const Cx<T> r = rho[n];
+    if (th.g == 0) return cx<T>(-r.x * a.A * sy, -r.y * a.A * sy);
+    return cx<T>(r.x * a.A * sin(a.kf * ((T)(2 * n) * a.dx)), r.y * a.A * sin(a.kf * ((T)(2 * n + 1) * a.dx)));
+  });
+  Cx<T>* xo = (th.g == 0 ? a.Xfx : a.Xfy) + ro;
+  row_r2c_finish<RF>(xs, th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
+}
+
+// ---------------------------------------------------------------- row pass 2
+// Groups: d(ux)/dx, d(uy)/dy, Bx, By [, dBy/dx, dBx/dy when corrected]; then
+// curl B; then three r2c (energy-flux curl terms and E_Visc).
 template <class T> struct RowCom2Args {
   Tables<T> tb;
   const Cx<T>* Xux;
@@ -129,78 +173,91 @@ template <class T> struct RowCom2Args {
   Cx<T>* Xey;
   Cx<T>* Xev;
   T eta, inv_nx;
-  int fix_curlB, rb;
+  int rb;
 };
 
-template <class T, int M, int P>
-__global__ void __launch_bounds__(128) k_row_com2(const RowCom2Args<T> a) {
+template <class T, int M, int P, int FIX>
+__global__ void __launch_bounds__(TARA_ROW_LB((FIX ? 6 : 4) * (M / P)),
+                                  TARA_MINB(TARA_ROW_LB((FIX ? 6 : 4) * (M / P))))
+k_row_com2(const RowCom2Args<T> a) {
   using RF = RowFFT<M, P>;
-  constexpr int NTR = M / P;
+  constexpr int NTR = M / P, G = FIX ? 6 : 4, NA = FIX ? 6 : 5, ARR = RF::SMEM_ELEMS;
   extern __shared__ __align__(16) unsigned char smraw[];
-  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
-  const int r = threadIdx.x / NTR, lane = threadIdx.x % NTR;
-  const int y = blockIdx.x * a.rb + r;
+  const RowThread<NTR, G> th;
+  const auto sync = th.sync();
   const Tables<T>& tb = a.tb;
-  Cx<T>* xs = sm + (size_t)r * 6 * M;
-  Cx<T>* dux = xs + M;
-  Cx<T>* duy = xs + 2 * M;
-  Cx<T>* bx = xs + 3 * M;
-  Cx<T>* by = xs + 4 * M;
-  Cx<T>* curl = xs + 5 * M;
+  Cx<T>* base = reinterpret_cast<Cx<T>*>(smraw) + (size_t)th.row * NA * ARR;
+  Cx<T>* dux = base;
+  Cx<T>* duy = base + ARR;
+  Cx<T>* bx = base + 2 * ARR;
+  Cx<T>* by = base + 3 * ARR;
+  Cx<T>* curl = base + 4 * ARR;
+  Cx<T>* aux = base + (NA - 1) * ARR;  // dBx/dy when corrected
+  const int y = blockIdx.x * a.rb + th.row;
   const size_t ro = (size_t)y * tb.ld;
   const T* kx = tb.kx;
   Cx<T> v[P];
-  // d_ux_dx = c2r(i kx ux_k)/(Nx Ny): on a row this is c2r_x(i kx X(ux))/Nx   (:164, :183)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ikmul(__ldg(kx + k), ldg(a.Xux + ro + k)); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) { dux[n] = cx<T>(z.x * a.inv_nx, z.y * a.inv_nx); });
-  // d_uy_dy                                                                    (:167, :184)
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(a.Hduy + ro + k); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) { duy[n] = cx<T>(normalise(z.x, tb), normalise(z.y, tb)); });
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(a.Hbx + ro + k); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) { bx[n] = cx<T>(normalise(z.x, tb), normalise(z.y, tb)); });
-  row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(a.Hby + ro + k); });
-  fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) { by[n] = cx<T>(normalise(z.x, tb), normalise(z.y, tb)); });
-  if (!a.fix_curlB) {
-    // d_Bx_dy = d_ux_dx/(NxNy), d_By_dx = d_uy_dy/(NxNy), curl = d_By_dx - d_Bx_dy   (:186-190)
-    fft_emit<RF>(lane, v, [&](int, int n, Cx<T>) {
-      const Cx<T> p = dux[n], q = duy[n];
-      curl[n] = cx<T>(q.x / tb.nn - p.x / tb.nn, q.y / tb.nn - p.y / tb.nn);
-    });
-  } else {
-    row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ikmul(__ldg(kx + k), ldg(a.Hby + ro + k)); });
-    fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) { curl[n] = cx<T>(normalise(z.x, tb), normalise(z.y, tb)); });
-    row_c2r<RF>(xs, lane, v, tb, [&](int k) { return ldg(a.Hikybx + ro + k); });
-    fft_emit<RF>(lane, v, [&](int, int n, Cx<T> z) {
-      const Cx<T> c = curl[n];
-      curl[n] = cx<T>(c.x - normalise(z.x, tb), c.y - normalise(z.y, tb));
+  // phase 1                                                              (:164-187)
+  {
+    const int g = th.g;
+    Cx<T>* dst = g == 0 ? dux : g == 1 ? duy : g == 2 ? bx : g == 3 ? by : g == 4 ? curl : aux;
+    row_c2r<RF>(dst, th.lane, v, tb, [&](int k) -> Cx<T> {
+      switch (g) {
+        case 0: return ikmul(__ldg(kx + k), ldg(a.Xux + ro + k));  // d_ux_dx: c2r_x(i kx X(ux))/Nx
+        case 1: return ldg(a.Hduy + ro + k);
+        case 2: return ldg(a.Hbx + ro + k);
+        case 3: return ldg(a.Hby + ro + k);
+        case 4: return ikmul(__ldg(kx + k), ldg(a.Hby + ro + k));  // d_By_dx (corrected)
+        default: return ldg(a.Hikybx + ro + k);                     // d_Bx_dy (corrected)
+      }
+    }, sync);
+    sync();
+    const T sc = g == 0 ? a.inv_nx : (T)1;
+    fft_emit<RF>(th.lane, v, [&](int, int n, Cx<T> z) {
+      dst[n] = g == 0 ? cx<T>(z.x * sc, z.y * sc) : cx<T>(normalise(z.x, tb), normalise(z.y, tb));
     });
   }
   __syncthreads();
+  // phase 2: curl B                                                      (:186-190)
+  for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
+    if (!FIX) {
+      // d_Bx_dy = d_ux_dx/(NxNy), d_By_dx = d_uy_dy/(NxNy)   (reference defect)
+      const Cx<T> p = dux[n], q = duy[n];
+      curl[n] = cx<T>(q.x / tb.nn - p.x / tb.nn, q.y / tb.nn - p.y / tb.nn);
+    } else {
+      const Cx<T> p = curl[n], q = aux[n];
+      curl[n] = cx<T>(p.x - q.x, p.y - q.y);
+    }
+  }
+  __syncthreads();
+  // phase 3: Energy_x -= eta By curl, Energy_y += eta Bx curl, E_Visc = (div u)^2   (:204-209)
   const T eta = a.eta;
-  // Energy_x -= eta By curl_B ; Energy_y += eta Bx curl_B ; E_Visc = (div u)^2   (:204-209)
-  Cx<T>* xex = a.Xex + ro;
-  Cx<T>* xey = a.Xey + ro;
-  Cx<T>* xev = a.Xev + ro;
-  row_r2c<RF>(xs, lane, NTR, v, tb,
-              [&](int n) {
-                const Cx<T> b = by[n], c = curl[n];
-                return cx<T>(-(eta * b.x * c.x), -(eta * b.y * c.y));
-              },
-              [&](int k, Cx<T> X) { st(xex + k, ld(xex + k) + X); });
-  row_r2c<RF>(xs, lane, NTR, v, tb,
-              [&](int n) {
-                const Cx<T> b = bx[n], c = curl[n];
-                return cx<T>(eta * b.x * c.x, eta * b.y * c.y);
-              },
-              [&](int k, Cx<T> X) { st(xey + k, ld(xey + k) + X); });
-  row_r2c<RF>(xs, lane, NTR, v, tb,
-              [&](int n) {
-                const Cx<T> p = dux[n], q = duy[n];
-                const T d0 = p.x + q.x, d1 = p.y + q.y;
-                return cx<T>(d0 * d0, d1 * d1);
-              },
-              [&](int k, Cx<T> X) { st(xev + k, X); });
+  if (th.g < 3) {
+    const int g = th.g;
+    row_r2c_begin<RF>(th.lane, v, tb, [&](int n) -> Cx<T> {
+      if (g == 0) {
+        const Cx<T> b = by[n], c = curl[n];
+        return cx<T>(-(eta * b.x * c.x), -(eta * b.y * c.y));
+      }
+      if (g == 1) {
+        const Cx<T> b = bx[n], c = curl[n];
+        return cx<T>(eta * b.x * c.x, eta * b.y * c.y);
+      }
+      const Cx<T> p = dux[n], q = duy[n];
+      const T d0 = p.x + q.x, d1 = p.y + q.y;
+      return cx<T>(d0 * d0, d1 * d1);
+    });
+  }
+  __syncthreads();  // inputs gathered: arrays 0..2 become exchange buffers
+  if (th.g < 3) {
+    const int g = th.g;
+    Cx<T>* xo = (g == 0 ? a.Xex : g == 1 ? a.Xey : a.Xev) + ro;
+    row_r2c_finish<RF>(base + g * ARR, th.lane, NTR, v, tb, [&](int k, Cx<T> X) {
+      st(xo + k, g == 2 ? X : ld(xo + k) + X);
+    }, sync);
+  }
 }
+
 
 template <class T> struct ColFwdComArgs {
   Tables<T> tb;
@@ -212,7 +269,7 @@ template <class T> struct ColFwdComArgs {
 };
 
 template <class T, int L, int CB, int P>
-__global__ void __launch_bounds__(CB * L / P) k_col_fwd_com(const ColFwdComArgs<T> a) {
+__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_com(const ColFwdComArgs<T> a) {
   using F = FFTB<L, CB, P>;
   constexpr int RL = F::Pl::R[F::S - 1];
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -308,9 +365,9 @@ __global__ void __launch_bounds__(CB * L / P) k_col_fwd_com(const ColFwdComArgs<
 
 template <int L, class T>
 inline void col_fwd_com_dispatch(const ColFwdComArgs<T>& a, cudaStream_t st) {
-  constexpr int CB = ColCfg<T, L>::CB, P = ColCfg<T, L>::P;
+  constexpr int CB = ColFwdComCfg<T, L>::CB, P = ColFwdComCfg<T, L>::P;
   auto kern = k_col_fwd_com<T, L, CB, P>;
-  const size_t smem = col_smem_bytes<T, L>();
+  const size_t smem = (size_t)FFTB<L, CB, P>::SMEM_ELEMS * sizeof(Cx<T>);
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid((a.tb.Nh + CB - 1) / CB, 6);
   kern<<<grid, CB * L / P, smem, st>>>(a);
@@ -322,31 +379,50 @@ static void launch_row_com1(const RowCom1Args<T>& a0, int Ny, cudaStream_t st) {
   constexpr int P = RowCfg<M>::P;
   constexpr int NTR = M / P;
   RowCom1Args<T> a = a0;
-  const size_t per_row = (size_t)9 * M * sizeof(Cx<T>);
-  a.rb = rows_per_cta(NTR, Ny, per_row);
+  const size_t per_row = (size_t)8 * RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<T>);
+  a.rb = row_cta_rows(8 * NTR, per_row, Ny);
   auto kern = k_row_com1<T, M, P>;
   const size_t smem = per_row * a.rb;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<Ny / a.rb, NTR * a.rb, smem, st>>>(a);
+  kern<<<Ny / a.rb, 8 * NTR * a.rb, smem, st>>>(a);
 }
 template <int Nx, class T>
-static void launch_row_com2(const RowCom2Args<T>& a0, int Ny, cudaStream_t st) {
+static void launch_row_force(const RowForceArgs<T>& a0, int Ny, cudaStream_t st) {
   constexpr int M = Nx / 2;
   constexpr int P = RowCfg<M>::P;
   constexpr int NTR = M / P;
-  RowCom2Args<T> a = a0;
-  const size_t per_row = (size_t)6 * M * sizeof(Cx<T>);
-  a.rb = rows_per_cta(NTR, Ny, per_row);
-  auto kern = k_row_com2<T, M, P>;
+  RowForceArgs<T> a = a0;
+  const size_t per_row = (size_t)3 * RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<T>);
+  a.rb = row_cta_rows(2 * NTR, per_row, Ny);
+  auto kern = k_row_force<T, M, P>;
   const size_t smem = per_row * a.rb;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<Ny / a.rb, NTR * a.rb, smem, st>>>(a);
+  kern<<<Ny / a.rb, 2 * NTR * a.rb, smem, st>>>(a);
+}
+template <int FIX, int Nx, class T>
+static void launch_row_com2_t(const RowCom2Args<T>& a0, int Ny, cudaStream_t st) {
+  constexpr int M = Nx / 2;
+  constexpr int P = RowCfg<M>::P;
+  constexpr int NTR = M / P;
+  constexpr int G = FIX ? 6 : 4, NA = FIX ? 6 : 5;
+  RowCom2Args<T> a = a0;
+  const size_t per_row = (size_t)NA * RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<T>);
+  a.rb = row_cta_rows(G * NTR, per_row, Ny);
+  auto kern = k_row_com2<T, M, P, FIX>;
+  const size_t smem = per_row * a.rb;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<Ny / a.rb, G * NTR * a.rb, smem, st>>>(a);
+}
+template <int Nx, class T>
+static void launch_row_com2(const RowCom2Args<T>& a, int Ny, int fix, cudaStream_t st) {
+  if (fix) launch_row_com2_t<1, Nx>(a, Ny, st);
+  else launch_row_com2_t<0, Nx>(a, Ny, st);
 }
 
 template <class T>
 int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* const in[6],
             const StepArgs<T>& step, cudaStream_t st) {
-  if ((size_t)9 * (g.Nx / 2) * sizeof(Cx<T>) > 227 * 1024) {
+  if ((size_t)8 * (g.Nx / 2 + g.Nx / 32 + 1) * sizeof(Cx<T>) > 227 * 1024 || 8 * (g.Nx / 2) / 16 > 1024) {
     set_error("MHD row pass does not fit in shared memory at this Nx and precision");
     return TARA_EUNSUPPORTED;
   }
@@ -364,13 +440,21 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   for (int q = 0; q < 6; q++) r1.H[q] = w.H[q];
   for (int q = 0; q < 11; q++) r1.X[q] = w.X[q];
   r1.cs2 = p.cs2;
-  r1.A = p.A;
-  r1.kf = p.kf;
-  r1.dx = (T)(g.Lx / g.Nx);
-  r1.dy = (T)(g.Ly / g.Ny);
-  r1.forcing = forcing;
   prof_mark(g.prof, st, KK_ROW_COM1);
   TARA_DISPATCH_LEN(g.Nx, launch_row_com1, r1, g.Ny, st)
+  if (forcing) {
+    RowForceArgs<T> rf{};
+    rf.tb = g.tb;
+    rf.Hrho = w.H[HRHO];
+    rf.Xfx = w.X[XFX];
+    rf.Xfy = w.X[XFY];
+    rf.A = p.A;
+    rf.kf = p.kf;
+    rf.dx = (T)(g.Lx / g.Nx);
+    rf.dy = (T)(g.Ly / g.Ny);
+    prof_mark(g.prof, st, KK_ROW_FORCE);
+    TARA_DISPATCH_LEN(g.Nx, launch_row_force, rf, g.Ny, st)
+  }
 
   ColRtArgs<T> rt{};
   rt.tb = g.tb;
@@ -392,9 +476,8 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   r2.Xev = w.X[XEV];
   r2.eta = p.eta;
   r2.inv_nx = (T)(1.0 / g.Nx);
-  r2.fix_curlB = p.fix_curlB;
   prof_mark(g.prof, st, KK_ROW_COM2);
-  TARA_DISPATCH_LEN(g.Nx, launch_row_com2, r2, g.Ny, st)
+  TARA_DISPATCH_LEN(g.Nx, launch_row_com2, r2, g.Ny, p.fix_curlB, st)
 
   ColFwdComArgs<T> cf{};
   cf.tb = g.tb;

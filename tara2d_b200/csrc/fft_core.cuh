@@ -201,6 +201,7 @@ TARA_PLAN(256, 8, 3, 8, 8, 4, 1)
 TARA_PLAN(512, 8, 3, 8, 8, 8, 1)
 TARA_PLAN(1024, 8, 4, 8, 8, 8, 2)
 TARA_PLAN(2048, 8, 4, 8, 8, 8, 4)
+TARA_PLAN(4096, 8, 4, 8, 8, 8, 8)
 TARA_PLAN(16, 16, 1, 16, 1, 1, 1)
 TARA_PLAN(32, 16, 2, 16, 2, 1, 1)
 TARA_PLAN(64, 16, 2, 16, 4, 1, 1)

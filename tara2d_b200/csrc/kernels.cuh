@@ -16,11 +16,21 @@ template <int L> struct ColCfg<float, L> {
   static constexpr int P = (L == 384) ? 24 : 16;
   static constexpr int CB = (L <= 1024) ? 8 : 4;
 };
+// Column pass of the MHD epilogue (two live value sets per thread: the FFT
+// and the derivative being assembled), so fewer values per thread.
+template <class T, int L> struct ColFwdComCfg { static constexpr int CB = 4, P = 16; };
+template <int L> struct ColFwdComCfg<double, L> {
+  static constexpr int P = (L == 384) ? 24 : (L >= 512 ? 8 : 16);
+  static constexpr int CB = (L <= 256) ? 8 : (L == 384 ? 4 : 2);
+};
+template <int L> struct ColFwdComCfg<float, L> {
+  static constexpr int P = (L == 384) ? 24 : (L >= 512 ? 8 : 16);
+  static constexpr int CB = (L <= 256) ? 8 : 4;
+};
 // Row pass: P values per thread (M = Nx/2 points per row FFT).
 template <int M> struct RowCfg { static constexpr int P = 16; };
 template <> struct RowCfg<8> { static constexpr int P = 8; };
 template <> struct RowCfg<192> { static constexpr int P = 24; };
-template <> struct RowCfg<512> { static constexpr int P = 8; };
 
 #define TARA_DISPATCH_LEN(n, FN, ...)                    \
   switch (n) {                                           \
@@ -36,6 +46,13 @@ template <> struct RowCfg<512> { static constexpr int P = 8; };
     case 4096: FN<4096>(__VA_ARGS__); break;             \
     default: break;                                      \
   }
+
+// Minimum resident CTAs per SM requested from the register allocator: at
+// least 16 warps per SM for CTAs of up to 256 threads.
+#define TARA_MINB(nt) ((nt) <= 128 ? 4 : ((nt) <= 256 ? 2 : 1))
+// Launch bound of a row kernel whose rows need tpr threads each: small rows
+// are packed several per CTA up to 128 threads.
+#define TARA_ROW_LB(tpr) ((tpr) >= 128 ? ((tpr) <= 1024 ? (tpr) : 1024) : 128)
 
 // ------------------------------------------------------------ multipliers
 enum : int { MUL_ONE = 0, MUL_IKY = 1, MUL_KY2 = 2 };
@@ -60,7 +77,7 @@ template <class T> struct ColInvArgs {
 
 // blockIdx.x: tile of CB kx columns; blockIdx.y: job
 template <class T, int L, int CB, int P>
-__global__ void __launch_bounds__(CB * L / P) k_col_inv(const ColInvArgs<T> a) {
+__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_inv(const ColInvArgs<T> a) {
   using F = FFTB<L, CB, P>;
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
@@ -149,7 +166,7 @@ template <class T> struct ColFwdSimpleArgs {
 };
 
 template <class T, int L, int CB, int P>
-__global__ void __launch_bounds__(CB * L / P) k_col_fwd_simple(const ColFwdSimpleArgs<T> a) {
+__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_simple(const ColFwdSimpleArgs<T> a) {
   using F = FFTB<L, CB, P>;
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
@@ -176,7 +193,7 @@ __global__ void __launch_bounds__(CB * L / P) k_col_fwd_simple(const ColFwdSimpl
 
 template <class T, int L>
 inline size_t col_smem_bytes() {
-  return (size_t)ColCfg<T, L>::CB * L * sizeof(Cx<T>);
+  return (size_t)FFTB<L, ColCfg<T, L>::CB, ColCfg<T, L>::P>::SMEM_ELEMS * sizeof(Cx<T>);
 }
 
 template <class T, int L>
@@ -229,7 +246,7 @@ template <class T> struct ColRtArgs {
   int mul;
 };
 template <class T, int L, int CB, int P>
-__global__ void __launch_bounds__(CB * L / P) k_col_rt(const ColRtArgs<T> a) {
+__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_rt(const ColRtArgs<T> a) {
   using F = FFTB<L, CB, P>;
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
@@ -243,9 +260,9 @@ __global__ void __launch_bounds__(CB * L / P) k_col_rt(const ColRtArgs<T> a) {
     return ldg(a.src + (size_t)i * ld + c);
   }, SyncBlock{});
   __syncthreads();
-  fft_emit<F>(threadIdx.x, v, [&](int t, int j, Cx<T> x) { sm[j * CB + t] = apply_ymul(a.mul, __ldg(ky + j), x); });
+  fft_emit<F>(threadIdx.x, v, [&](int t, int j, Cx<T> x) { sm[F::sidx(t, j)] = apply_ymul(a.mul, __ldg(ky + j), x); });
   __syncthreads();
-  fft_run<F, +1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) { return sm[i * CB + t]; },
+  fft_run<F, +1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) { return sm[F::sidx(t, i)]; },
                  SyncBlock{});
   fft_emit<F>(threadIdx.x, v, [&](int t, int i, Cx<T> x) {
     const int c = c0 + t;

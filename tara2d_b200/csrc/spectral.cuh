@@ -63,13 +63,22 @@ template <class T> __device__ __forceinline__ T normalise(T x, const Tables<T>& 
   return tb.nn_pow2 ? x * tb.inv_nn : x / tb.nn;
 }
 
+// BatchFFT with its shared-memory exchange layout.  Element (t, i) lives at
+// sidx(t, i) = i*B + t + i/R0: one pad slot every R0 rows breaks the bank
+// conflicts of the first stage's stores (stride R0 between neighbouring
+// butterflies).
+template <int L, int B, int P> struct FFTB : BatchFFT<L, B, P> {
+  static constexpr int B_ = B;
+  static constexpr int L_ = L;
+  static constexpr int PADR = BatchFFT<L, B, P>::Pl::R[0];
+  static constexpr int SMEM_ELEMS = L * B + L / PADR + 1;
+  __host__ __device__ static constexpr int sidx(int t, int i) { return i * B + t + i / PADR; }
+};
+template <int L, int P> using RowFFT = FFTB<L, 1, P>;
+
 // ------------------------------------------------------------------ stages
-// Generic driver of one batched FFT whose intermediate stages go through the
-// shared-memory tile `sm` (element (t, i) at sm[i*B + t]).  `pro(t, i)`
-// supplies stage-0 input (t, i); `epi(t, i, v)` consumes output (t, i).
-// All threads of the group must call it (it contains barriers via SYNC).
-template <class F, int s, class T, class SYNC>
-__device__ __forceinline__ void fft_store(Cx<T>* sm, int tid, const Cx<T>* v, SYNC sync) {
+template <class F, int s, class T>
+__device__ __forceinline__ void fft_store(Cx<T>* sm, int tid, const Cx<T>* v) {
   constexpr int R = F::Pl::R[s];
 #pragma unroll
   for (int q = 0; q < F::P / R; q++)
@@ -77,7 +86,7 @@ __device__ __forceinline__ void fft_store(Cx<T>* sm, int tid, const Cx<T>* v, SY
     for (int r = 0; r < R; r++) {
       int t, i;
       F::template out_pos<s>(tid, q, r, t, i);
-      sm[i * F::B_ + t] = v[q * R + r];
+      sm[F::sidx(t, i)] = v[q * R + r];
     }
 }
 template <class F, int s, class T>
@@ -89,25 +98,24 @@ __device__ __forceinline__ void fft_load(const Cx<T>* sm, int tid, Cx<T>* v) {
     for (int r = 0; r < R; r++) {
       int t, i;
       F::template in_pos<s>(tid, q, r, t, i);
-      v[q * R + r] = sm[i * F::B_ + t];
+      v[q * R + r] = sm[F::sidx(t, i)];
     }
 }
+// Stages s..S-1 (s >= 1); the values of stage s-1 are in v.
 template <class F, int s, int DIR, class T, class TW, class SYNC>
 __device__ __forceinline__ void fft_rest(Cx<T>* sm, int tid, Cx<T>* v, const TW& tw, SYNC sync) {
   if constexpr (s < F::S) {
     sync();
-    fft_store<F, s - 1>(sm, tid, v, sync);
+    fft_store<F, s - 1>(sm, tid, v);
     sync();
     fft_load<F, s>(sm, tid, v);
     F::template compute<s, DIR>(tid, v, tw);
     fft_rest<F, s + 1, DIR>(sm, tid, v, tw, sync);
   }
 }
-
-// Runs the transform; on return v[] holds the outputs of the last stage for
-// this thread, positions given by F::out_pos<S-1>.
-template <class F, int DIR, class T, class TW, class PRO, class SYNC>
-__device__ __forceinline__ void fft_run(Cx<T>* sm, int tid, Cx<T>* v, const TW& tw, PRO&& pro, SYNC sync) {
+// Stage-0 inputs from pro(t, i), stage-0 butterflies.
+template <class F, int DIR, class T, class TW, class PRO>
+__device__ __forceinline__ void fft_begin(int tid, Cx<T>* v, const TW& tw, PRO&& pro) {
   constexpr int R0 = F::Pl::R[0];
 #pragma unroll
   for (int q = 0; q < F::P / R0; q++)
@@ -118,6 +126,13 @@ __device__ __forceinline__ void fft_run(Cx<T>* sm, int tid, Cx<T>* v, const TW& 
       v[q * R0 + r] = pro(t, i);
     }
   F::template compute<0, DIR>(tid, v, tw);
+}
+// The whole transform; on return v[] holds the last stage's outputs
+// (positions F::out_pos<S-1>).  `sync` must synchronise every thread that
+// shares `sm`.
+template <class F, int DIR, class T, class TW, class PRO, class SYNC>
+__device__ __forceinline__ void fft_run(Cx<T>* sm, int tid, Cx<T>* v, const TW& tw, PRO&& pro, SYNC sync) {
+  fft_begin<F, DIR>(tid, v, tw, pro);
   fft_rest<F, 1, DIR>(sm, tid, v, tw, sync);
 }
 template <class F, class T, class EPI>
@@ -133,13 +148,45 @@ __device__ __forceinline__ void fft_emit(int tid, const Cx<T>* v, EPI&& epi) {
     }
 }
 
-// BatchFFT with the batch size exposed for the smem layout.
-template <int L, int B, int P> struct FFTB : BatchFFT<L, B, P> {
-  static constexpr int B_ = B;
-};
-
 struct SyncBlock {
   __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+// Barrier of one group of NTR consecutive threads: __syncwarp over the
+// group's lanes for NTR <= 32 (groups sharing a warp synchronise
+// independently), else named barrier `id` (1..15) of NTR threads.
+template <int NTR> struct SyncGroup {
+  int id;
+  unsigned mask;
+  __device__ __forceinline__ void operator()() const {
+    if constexpr (NTR <= 32) {
+      __syncwarp(mask);
+    } else {
+      asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(NTR) : "memory");
+    }
+  }
+};
+
+// Thread geometry of a row kernel: RB rows per CTA, G groups of NTR threads
+// per row; each group runs one row FFT at a time.
+template <int NTR, int G> struct RowThread {
+  int row, g, lane, gid;
+  __device__ __forceinline__ RowThread() {
+    const int t = threadIdx.x;
+    lane = t % NTR;
+    gid = t / NTR;
+    g = gid % G;
+    row = gid / G;
+  }
+  __device__ __forceinline__ SyncGroup<NTR> sync() const {
+    SyncGroup<NTR> s;
+    s.id = 1 + gid;
+    if constexpr (NTR < 32) {
+      s.mask = ((1u << NTR) - 1u) << ((threadIdx.x & 31) / NTR * NTR);
+    } else {
+      s.mask = 0xffffffffu;
+    }
+    return s;
+  }
 };
 
 // ----------------------------------------------------------- row helpers
@@ -147,8 +194,9 @@ struct SyncBlock {
 // hv(k) returns X[k] for 0 < k < M; for k = 0 and k = M only its real part
 // is used (the kx = 0 / Nyquist bins of a c2r).  On return the thread holds
 // z[n] = x[2n] + i x[2n+1] for its output positions n (RowF::out_pos).
-template <class RowF, class T, class HV>
-__device__ __forceinline__ void row_c2r(Cx<T>* xs, int lane, Cx<T>* v, const Tables<T>& tb, HV&& hv) {
+// xs: exchange buffer of RowF::SMEM_ELEMS elements private to the group.
+template <class RowF, class T, class HV, class SYNC>
+__device__ __forceinline__ void row_c2r(Cx<T>* xs, int lane, Cx<T>* v, const Tables<T>& tb, HV&& hv, SYNC sync) {
   constexpr int M = RowF::L_;
   TwGlobal<T> tw{tb.tw_row};
   fft_run<RowF, +1>(xs, lane, v, tw, [&](int, int i) -> Cx<T> {
@@ -164,24 +212,30 @@ __device__ __forceinline__ void row_c2r(Cx<T>* xs, int lane, Cx<T>* v, const Tab
     Cx<T> w = ldg(tb.tw_real + i);  // e^{-2 pi i i/N}
     Cx<T> fo = cmul(A - B, conj(w));
     return cx<T>(fe.x - fo.y, fe.y + fo.x);
-  }, SyncBlock{});
+  }, sync);
 }
 
-// Forward real transform of one row: x[0..2M-1] -> X[0..M].
-// gv(n) returns z[n] = x[2n] + i x[2n+1]; out(k, X) is called for k = 0..M
-// (X[0], X[M] real).  zs is an M-element smem buffer private to the row.
-template <class RowF, class T, class GV, class OUT>
-__device__ __forceinline__ void row_r2c(Cx<T>* zs, int lane, int ntr, Cx<T>* v, const Tables<T>& tb,
-                                        GV&& gv, OUT&& out) {
+// Forward real transform of one row, x[0..2M-1] -> X[0..M], in two parts so
+// that the inputs can be gathered before the exchange buffer is claimed:
+//   row_r2c_begin: gv(n) returns z[n] = x[2n] + i x[2n+1] at the stage-0
+//                  positions; stage-0 butterflies;
+//   row_r2c_finish: remaining stages in `zs`, then the real-to-complex
+//                  post-processing; out(k, X) for k = 0..M (X[0], X[M] real).
+template <class RowF, class T, class GV>
+__device__ __forceinline__ void row_r2c_begin(int lane, Cx<T>* v, const Tables<T>& tb, GV&& gv) {
+  fft_begin<RowF, -1>(lane, v, TwGlobal<T>{tb.tw_row}, [&](int, int i) { return gv(i); });
+}
+template <class RowF, class T, class OUT, class SYNC>
+__device__ __forceinline__ void row_r2c_finish(Cx<T>* zs, int lane, int ntr, Cx<T>* v, const Tables<T>& tb,
+                                               OUT&& out, SYNC sync) {
   constexpr int M = RowF::L_;
-  TwGlobal<T> tw{tb.tw_row};
-  fft_run<RowF, -1>(zs, lane, v, tw, [&](int, int i) { return gv(i); }, SyncBlock{});
-  __syncthreads();
-  fft_emit<RowF>(lane, v, [&](int, int i, Cx<T> z) { zs[i] = z; });
-  __syncthreads();
+  fft_rest<RowF, 1, -1>(zs, lane, v, TwGlobal<T>{tb.tw_row}, sync);
+  sync();
+  fft_emit<RowF>(lane, v, [&](int, int i, Cx<T> z) { zs[RowF::sidx(0, i)] = z; });
+  sync();
   for (int k = lane; k <= M; k += ntr) {
-    Cx<T> zk = zs[k == M ? 0 : k];
-    Cx<T> zm = conj(zs[k == 0 ? 0 : M - k]);
+    Cx<T> zk = zs[RowF::sidx(0, k == M ? 0 : k)];
+    Cx<T> zm = conj(zs[RowF::sidx(0, k == 0 ? 0 : M - k)]);
     Cx<T> e = rmul((T)0.5, zk + zm);
     Cx<T> d = zk - zm;
     Cx<T> o = cx<T>((T)0.5 * d.y, (T)-0.5 * d.x);  // (zk - zm)/(2i)
@@ -191,9 +245,5 @@ __device__ __forceinline__ void row_r2c(Cx<T>* zs, int lane, int ntr, Cx<T>* v, 
     out(k, X);
   }
 }
-
-template <int L, int P> struct RowFFT : FFTB<L, 1, P> {
-  static constexpr int L_ = L;
-};
 
 }  // namespace tara
