@@ -88,17 +88,20 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
   const T cs2 = a.cs2;
   const int q = th.g;
   row_r2c_begin<RF>(th.lane, v, tb, [&](int n) -> Cx<T> {
+    Cx<T> F[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) F[k] = f[k][n];
     T o[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
-      const T rho = h ? f[0][n].y : f[0][n].x;
-      const T mx = h ? f[1][n].y : f[1][n].x;
-      const T my = h ? f[2][n].y : f[2][n].x;
-      const T E = h ? f[3][n].y : f[3][n].x;
-      const T bx = h ? f[4][n].y : f[4][n].x;
-      const T by = h ? f[5][n].y : f[5][n].x;
-      const T ux = h ? f[6][n].y : f[6][n].x;
-      const T uy = h ? f[7][n].y : f[7][n].x;
+      const T rho = h ? F[0].y : F[0].x;
+      const T mx = h ? F[1].y : F[1].x;
+      const T my = h ? F[2].y : F[2].x;
+      const T E = h ? F[3].y : F[3].x;
+      const T bx = h ? F[4].y : F[4].x;
+      const T by = h ? F[5].y : F[5].x;
+      const T ux = h ? F[6].y : F[6].x;
+      const T uy = h ? F[7].y : F[7].x;
       const T B2 = bx * bx + by * by;
       const T Pr = cs2 * rho;
       T r;

@@ -35,8 +35,10 @@
 
 namespace tara {
 
+// Aligned to its size so that shared/global accesses are single 16-byte
+// (double) or 8-byte (float) transactions.
 template <class T>
-struct Cx {
+struct alignas(2 * sizeof(T)) Cx {
   T x, y;
 };
 
@@ -268,11 +270,29 @@ template <int L, int B, int P_> struct BatchFFT {
         int j = b / B;
         int jm = j % Ns;
         constexpr int stride = L / (Ns * R);
+        // w^r for r = 1..R-1 from the table entries w^1, w^2, w^4, w^8 (at
+        // most two further products each, so within a few ulp of the table)
+        const int m1 = jm * stride;
+        Cx<T> w[16];
+        w[1] = tw(m1);
+        if constexpr (R >= 3) w[2] = tw(2 * m1);
+        if constexpr (R >= 4) w[3] = cmul(w[2], w[1]);
+        if constexpr (R >= 5) w[4] = tw(4 * m1);
+        if constexpr (R >= 6) w[5] = cmul(w[4], w[1]);
+        if constexpr (R >= 8) {
+          w[6] = cmul(w[4], w[2]);
+          w[7] = cmul(w[4], w[3]);
+        }
+        if constexpr (R >= 16) {
+          w[8] = tw(8 * m1);
+#pragma unroll
+          for (int r = 9; r < 16; r++) w[r] = cmul(w[8], w[r - 8]);
+        }
 #pragma unroll
         for (int r = 1; r < R; r++) {
-          Cx<T> w = tw(jm * r * stride);
-          if (DIR > 0) w.y = -w.y;
-          u[r] = cmul(u[r], w);
+          Cx<T> wr = w[r];
+          if (DIR > 0) wr.y = -wr.y;
+          u[r] = cmul(u[r], wr);
         }
       }
       dft<R, DIR>(u);
