@@ -122,6 +122,22 @@ int tara_derive2coh(const tara_params* p, int Nx, int Ny, const double* nk, cons
 int tara_derive2com(const tara_params* p, int Nx, int Ny, const double* const* state6,
                     double* const* rhs6);
 
+/* Hydro right-hand side that allocates nothing (no counterpart in the
+ * reference; it is an addition for hosts that must not allocate device
+ * memory from the solver, e.g. a program whose own pool allocator already
+ * holds all device memory, or a time-critical loop that cannot afford an
+ * allocation's latency and implicit synchronisation).  Same result as
+ * tara_derive2coh, but inputs and outputs are device buffers the caller owns
+ * (complex(8) (Nh,Ny), no padding) and every temporary lives in one static
+ * device workspace of about 6 MB reserved when the library loads.
+ * Nx, Ny must be 16, 32, 64, 128 or 256; anything larger returns
+ * TARA_EINVAL.  All calls share the workspace, so calls that overlap on the
+ * GPU race; calls on one stream are ordered.  The first call on a device
+ * looks up the workspace address and should come before any stream capture.
+ * `stream` is a cudaStream_t (NULL: the default stream). */
+int tara_derive2coh_noalloc(const tara_params* p, int Nx, int Ny, const double* nk, const double* ukx,
+                            const double* uky, double* dn_dt, double* dux_dt, double* duy_dt, void* stream);
+
 /* ---- drop-in Fortran entry points (reference signatures) ---------------- */
 /* src/derive2coh.f95:6-7 */
 void derive2coh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* pi,
