@@ -107,6 +107,9 @@ struct tara_session {
     if (s != TARA_OK && status == TARA_OK) status = s;
     return s;
   }
+  // Device status word: TARA_ETIMEOUT when a kernel's bounded wait ran out
+  // (the word is cleared after it has been reported).
+  virtual int device_status() = 0;
   // elementwise stepper on host fields (drop-in ab2/euler/pc/rk4 entry points);
   // nfld fields, each out = stepper(u, d1, d2)
   virtual int elementwise(int mode, int nfld, const double* const* u, const double* const* d1,
@@ -193,6 +196,20 @@ struct SessionT : tara_session {
 
   FieldPool<T>& pool(int which) { return which == 0 ? u : dold; }
 
+  int device_status() override {
+    int v = 0;
+    TARA_CUDA_TRY(cudaMemcpyAsync(&v, g.tb.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (v != TARA_OK) {
+      const int zero = 0;
+      cudaMemcpyAsync(g.tb.status, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+      cudaStreamSynchronize(st);
+      set_error("a bounded wait for a TMA tile load ran out in a kernel");
+      return v;
+    }
+    return TARA_OK;
+  }
+
   int h2d(const double* h, Cx<T>* d) {
     if (!h) { set_error("null host field pointer"); return TARA_EINVAL; }
     if constexpr (sizeof(T) == sizeof(double)) {
@@ -232,7 +249,7 @@ struct SessionT : tara_session {
   int get_fields(int which, double* const* h) override {
     if (!h) { set_error("null field array"); return TARA_EINVAL; }
     for (int f = 0; f < nf; f++) TARA_TRY(d2h(pool(which)[f], h[f]));
-    return TARA_OK;
+    return device_status();
   }
 
   int rhs(Cx<T>* const* in, const StepArgs<T>& s) {
@@ -262,7 +279,7 @@ struct SessionT : tara_session {
     for (int f = 0; f < nf; f++) in[f] = u[f];
     TARA_TRY(rhs(in, base_args(STEP_RHS)));
     for (int f = 0; f < nf; f++) TARA_TRY(d2h(tmp[f], out[f]));
-    return TARA_OK;
+    return device_status();
   }
   // One step reads the state from `u` and writes the new state to `unew`
   // (the RHS of one field reads other fields of its input state, so no
@@ -436,7 +453,7 @@ int tara_synchronize(tara_session* s) {
     set_error(std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e));
     return s->fail_if(TARA_ECUDA);
   }
-  return TARA_OK;
+  return s->fail_if(s->device_status());
 }
 int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms) {
   if (!s || !ms || nsteps < 0) return TARA_EINVAL;
@@ -451,6 +468,8 @@ int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms) {
     return s->fail_if(TARA_ECUDA);
   }
   cudaEventElapsedTime(ms, s->ev0, s->ev1);
+  r = s->device_status();
+  if (r != TARA_OK) return s->fail_if(r);
   return TARA_OK;
 }
 int tara_profile_steps(tara_session* s, int stepper, int nsteps, double* kernel_ms, int* kernel_launches,

@@ -2,6 +2,8 @@
 // step) and the launch configurations shared by every model.
 #pragma once
 #include "spectral.cuh"
+#include "tma.cuh"
+#include "../../include/tara2d_gpu.h"
 
 namespace tara {
 
@@ -95,6 +97,88 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_inv(c
     const int c = c0 + t;
     if (c < Nh) st(jb.dst + (size_t)i * ld + c, x);
   });
+}
+
+// TMA-staged, persistent variant: each CTA loops over (tile, job) items; the
+// next item's column tile is loaded by the TMA unit into the other of two
+// shared-memory buffers while the current one is transformed in place.
+template <class T> struct ColInvTmaArgs {
+  ColInvJob<T> job[8];
+  CUtensorMap map[8];
+  Tables<T> tb;
+  int njobs, ntiles;
+};
+
+template <int L, int CB, int P> struct ColTmaLayout {
+  using F = FFTB<L, CB, P>;
+  static constexpr int BOX = L <= 256 ? L : (L % 256 == 0 ? 256 : 128);  // rows per TMA box (divides L)
+  static constexpr int BUFE = (F::SMEM_ELEMS + 7) / 8 * 8;  // complex elements per buffer (128-byte multiple)
+  template <class T> static constexpr size_t bytes() { return 2 * (size_t)BUFE * sizeof(Cx<T>) + 64; }
+};
+
+template <class T, int L, int CB, int P>
+__global__ void __launch_bounds__(CB * L / P, 1) k_col_inv_tma(const __grid_constant__ ColInvTmaArgs<T> a) {
+  using F = FFTB<L, CB, P>;
+  using LY = ColTmaLayout<L, CB, P>;
+  constexpr unsigned TILE_BYTES = (unsigned)(CB * L * sizeof(Cx<T>));
+  extern __shared__ __align__(128) unsigned char smraw[];
+  Cx<T>* buf0 = reinterpret_cast<Cx<T>*>(smraw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + 2 * (size_t)LY::BUFE * sizeof(Cx<T>));
+  const int tid = threadIdx.x;
+  const int nitems = a.ntiles * a.njobs;
+  const int Nh = a.tb.Nh, ld = a.tb.ld;
+  const T* ky = a.tb.ky;
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  auto issue = [&](int item, int b) {
+    const int job = item % a.njobs, tile = item / a.njobs;
+    Cx<T>* dst = buf0 + b * LY::BUFE;
+    mbar_expect_tx(&bars[b], TILE_BYTES);
+#pragma unroll 1
+    for (int y = 0; y < L; y += LY::BOX) tma_load_2d(dst + y * CB, &a.map[job], 2 * tile * CB, y, &bars[b]);
+  };
+  int item = blockIdx.x;
+  if (tid == 0 && item < nitems) issue(item, 0);
+  int it = 0;
+  bool failed = false;
+  for (; item < nitems; item += gridDim.x, it++) {
+    const int b = it & 1;
+    const unsigned parity = (it >> 1) & 1;
+    const int next = item + gridDim.x;
+    if (tid == 0 && next < nitems) {
+      fence_proxy_async_smem();
+      issue(next, b ^ 1);
+    }
+    const bool ok = mbar_wait_bounded(&bars[b], parity);
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    const int job = item % a.njobs, tile = item / a.njobs;
+    const ColInvJob<T> jb = a.job[job];
+    Cx<T>* sm = buf0 + b * LY::BUFE;
+    const int c0 = tile * CB;
+    Cx<T> v[P];
+    fft_run<F, +1>(sm, tid, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
+      return apply_ymul(jb.mul, __ldg(ky + i), sm[i * CB + t]);
+    }, SyncBlock{});
+    fft_emit<F>(tid, v, [&](int t, int i, Cx<T> x) {
+      const int c = c0 + t;
+      if (c < Nh) st(jb.dst + (size_t)i * ld + c, x);
+    });
+    __syncthreads();  // all reads of this buffer are done before it is refilled
+  }
+  if (failed) {
+    // record the failure, then let the loads still in flight land (bounded)
+    if (tid == 0) atomicExch(a.tb.status, TARA_ETIMEOUT);
+    const int b = it & 1;
+    mbar_wait_bounded(&bars[b], (it >> 1) & 1);
+    if (item + (int)gridDim.x < nitems) mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1);
+  }
 }
 
 // ------------------------------------------------------------ time steppers
@@ -220,7 +304,30 @@ inline int launch_col_fwd_simple(const ColFwdSimpleArgs<T>& a, int nf, cudaStrea
 
 template <int L, class T>
 inline void col_inv_dispatch(const ColInvArgs<T>& a, int njobs, cudaStream_t st) {
-  launch_col_inv<T, L>(a, njobs, st);
+  constexpr int CB = ColCfg<T, L>::CB, P = ColCfg<T, L>::P;
+  using LY = ColTmaLayout<L, CB, P>;
+  ColInvTmaArgs<T> t{};
+  t.tb = a.tb;
+  t.njobs = njobs;
+  t.ntiles = (a.tb.Nh + CB - 1) / CB;
+  bool maps_ok = (a.tb.ld * sizeof(Cx<T>)) % 16 == 0 && (2 * CB * sizeof(T)) % 16 == 0;
+  for (int q = 0; q < njobs && maps_ok; q++) {
+    t.job[q] = a.job[q];
+    maps_ok = make_col_tile_map<T>(&t.map[q], a.job[q].src, a.tb.ld, a.tb.Ny, CB, LY::BOX) == TARA_OK;
+  }
+  if (!maps_ok) {  // layouts the TMA unit cannot describe use the register-staged kernel
+    launch_col_inv<T, L>(a, njobs, st);
+    return;
+  }
+  auto kern = k_col_inv_tma<T, L, CB, P>;
+  const size_t smem = LY::template bytes<T>();
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, CB * L / P, smem);
+  const int nitems = t.ntiles * njobs;
+  int grid = a.tb.sm_count * (per_sm > 0 ? per_sm : 1);
+  if (grid > nitems) grid = nitems;
+  kern<<<grid, CB * L / P, smem, st>>>(t);
 }
 template <int L, class T>
 inline void col_fwd_simple_dispatch(const ColFwdSimpleArgs<T>& a, int nf, cudaStream_t st) {

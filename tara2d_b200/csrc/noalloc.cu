@@ -148,6 +148,20 @@ extern "C" int tara_derive2coh_noalloc(const tara_params* p, int Nx, int Ny, con
   g.tb.nn = nn;
   g.tb.inv_nn = 1.0 / nn;
   g.tb.nn_pow2 = 1;  // every accepted size is a power of two
+  // status word of the kernels' bounded waits: the last 256 bytes of the table region
+  g.tb.status = reinterpret_cast<int*>(dtab + kTableBytes - 256);
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    set_error("tara_derive2coh_noalloc: device query failed");
+    return TARA_ECUDA;
+  }
+  g.tb.sm_count = sms;
+  const int zero = 0;
+  e = cudaMemcpyAsync(g.tb.status, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    set_error(std::string("tara_derive2coh_noalloc: status reset: ") + cudaGetErrorString(e));
+    return TARA_ECUDA;
+  }
 
   // fields of this grid packed back to back in the workspace
   const size_t fe = (size_t)Ny * Nh;

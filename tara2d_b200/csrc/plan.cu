@@ -3,6 +3,7 @@
 #include <cstring>
 #include <mutex>
 #include "plan.h"
+#include "tma.cuh"
 
 namespace tara {
 
@@ -105,7 +106,8 @@ int Grid<T>::init(int nx, int ny, double lx, double ly, double pi_, cudaStream_t
   size_t o_twc = 0, o_twr = o_twc + al(twc.size() * sizeof(Cx<T>)),
          o_twre = o_twr + al(twr.size() * sizeof(Cx<T>)),
          o_kx = o_twre + al(twre.size() * sizeof(Cx<T>)), o_ky = o_kx + al(kx.size() * sizeof(T)),
-         o_cut = o_ky + al(ky.size() * sizeof(T)), total = o_cut + al(cut.size() * sizeof(int));
+         o_cut = o_ky + al(ky.size() * sizeof(T)), o_status = o_cut + al(cut.size() * sizeof(int)),
+         total = o_status + 256;
   if (cudaMalloc(&dmem, total) != cudaSuccess) {
     dmem = nullptr;
     set_error("cudaMalloc of grid tables failed");
@@ -127,12 +129,45 @@ int Grid<T>::init(int nx, int ny, double lx, double ly, double pi_, cudaStream_t
   tb.kx = (const T*)(b + o_kx);
   tb.ky = (const T*)(b + o_ky);
   tb.cut = (const int*)(b + o_cut);
+  tb.status = (int*)(b + o_status);
+  int dev = 0, sms = 0;
+  TARA_CUDA_TRY(cudaGetDevice(&dev));
+  TARA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  tb.sm_count = sms;
   tb.Nx = nx; tb.Ny = ny; tb.Nh = Nh; tb.ld = ld;
   double nn = (double)nx * (double)ny;
   tb.nn = (T)nn;
   tb.inv_nn = (T)(1.0 / nn);
   long long inn = (long long)nx * ny;
   tb.nn_pow2 = (inn & (inn - 1)) == 0;
+  return TARA_OK;
+}
+
+int tma_encode_tile(CUtensorMap* map, CUtensorMapDataType dt, void* base, uint64_t inner_elems, uint64_t rows,
+                    uint64_t row_bytes, uint32_t box_inner, uint32_t box_rows) {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return TARA_ECUDA;
+  }
+  cuuint64_t dims[2] = {inner_elems, rows};
+  cuuint64_t strides[1] = {row_bytes};
+  cuuint32_t box[2] = {box_inner, box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(map, dt, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed with CUresult " + std::to_string((int)r));
+    return TARA_ECUDA;
+  }
   return TARA_OK;
 }
 

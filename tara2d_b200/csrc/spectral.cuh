@@ -33,6 +33,8 @@ struct Tables {
   T inv_nn;              // 1/(Nx*Ny)
   T nn;                  // Nx*Ny
   int nn_pow2;           // Nx*Ny is a power of two (so x*inv_nn == x/nn exactly)
+  int* status;           // device status word (TARA_ETIMEOUT after a bounded wait ran out)
+  int sm_count;          // multiprocessors of the device (persistent grids)
 };
 
 template <class T> __device__ __forceinline__ Cx<T> ldg(const Cx<T>* p);
