@@ -271,28 +271,50 @@ template <int L, int B, int P_> struct BatchFFT {
         int jm = j % Ns;
         constexpr int stride = L / (Ns * R);
         // w^r for r = 1..R-1 from the table entries w^1, w^2, w^4, w^8 (at
-        // most two further products each, so within a few ulp of the table)
+        // most two further products each, so within a few ulp of the table),
+        // applied as soon as each is formed to keep few of them live
         const int m1 = jm * stride;
-        Cx<T> w[16];
-        w[1] = tw(m1);
-        if constexpr (R >= 3) w[2] = tw(2 * m1);
-        if constexpr (R >= 4) w[3] = cmul(w[2], w[1]);
-        if constexpr (R >= 5) w[4] = tw(4 * m1);
-        if constexpr (R >= 6) w[5] = cmul(w[4], w[1]);
-        if constexpr (R >= 8) {
-          w[6] = cmul(w[4], w[2]);
-          w[7] = cmul(w[4], w[3]);
-        }
-        if constexpr (R >= 16) {
-          w[8] = tw(8 * m1);
-#pragma unroll
-          for (int r = 9; r < 16; r++) w[r] = cmul(w[8], w[r - 8]);
-        }
-#pragma unroll
-        for (int r = 1; r < R; r++) {
-          Cx<T> wr = w[r];
+        auto apply = [&](int r, Cx<T> wr) {
           if (DIR > 0) wr.y = -wr.y;
           u[r] = cmul(u[r], wr);
+        };
+        const Cx<T> w1 = tw(m1);
+        Cx<T> w8;
+        if constexpr (R >= 16) {
+          w8 = tw(8 * m1);
+          apply(8, w8);
+          apply(9, cmul(w8, w1));
+        }
+        apply(1, w1);
+        if constexpr (R >= 3) {
+          const Cx<T> w2 = tw(2 * m1);
+          apply(2, w2);
+          if constexpr (R >= 16) apply(10, cmul(w8, w2));
+          if constexpr (R >= 4) {
+            const Cx<T> w3 = cmul(w2, w1);
+            apply(3, w3);
+            if constexpr (R >= 16) apply(11, cmul(w8, w3));
+            if constexpr (R >= 5) {
+              const Cx<T> w4 = tw(4 * m1);
+              apply(4, w4);
+              if constexpr (R >= 16) apply(12, cmul(w8, w4));
+              if constexpr (R >= 6) {
+                const Cx<T> w5 = cmul(w4, w1);
+                apply(5, w5);
+                if constexpr (R >= 16) apply(13, cmul(w8, w5));
+              }
+              if constexpr (R >= 8) {
+                const Cx<T> w6 = cmul(w4, w2);
+                apply(6, w6);
+                const Cx<T> w7 = cmul(w4, w3);
+                apply(7, w7);
+                if constexpr (R >= 16) {
+                  apply(14, cmul(w8, w6));
+                  apply(15, cmul(w8, w7));
+                }
+              }
+            }
+          }
         }
       }
       dft<R, DIR>(u);

@@ -143,8 +143,7 @@ int Grid<T>::init(int nx, int ny, double lx, double ly, double pi_, cudaStream_t
   return TARA_OK;
 }
 
-int tma_encode_tile(CUtensorMap* map, CUtensorMapDataType dt, void* base, uint64_t inner_elems, uint64_t rows,
-                    uint64_t row_bytes, uint32_t box_inner, uint32_t box_rows) {
+static PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
   std::call_once(once, [] {
@@ -154,10 +153,31 @@ int tma_encode_tile(CUtensorMap* map, CUtensorMapDataType dt, void* base, uint64
         q == cudaDriverEntryPointSuccess)
       fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
   });
-  if (!fn) {
-    set_error("cuTensorMapEncodeTiled is not available from the driver");
+  if (!fn) set_error("cuTensorMapEncodeTiled is not available from the driver");
+  return fn;
+}
+
+int tma_encode_tile3(CUtensorMap* map, CUtensorMapDataType dt, void* base, uint64_t inner_elems, uint64_t rows,
+                     uint64_t nf, uint64_t row_bytes, uint64_t field_bytes, uint32_t box_inner, uint32_t box_rows) {
+  auto fn = tma_encoder();
+  if (!fn) return TARA_ECUDA;
+  cuuint64_t dims[3] = {inner_elems, rows, nf};
+  cuuint64_t strides[2] = {row_bytes, field_bytes};
+  cuuint32_t box[3] = {box_inner, box_rows, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = fn(map, dt, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (3D) failed with CUresult " + std::to_string((int)r));
     return TARA_ECUDA;
   }
+  return TARA_OK;
+}
+
+int tma_encode_tile(CUtensorMap* map, CUtensorMapDataType dt, void* base, uint64_t inner_elems, uint64_t rows,
+                    uint64_t row_bytes, uint32_t box_inner, uint32_t box_rows) {
+  auto fn = tma_encoder();
+  if (!fn) return TARA_ECUDA;
   cuuint64_t dims[2] = {inner_elems, rows};
   cuuint64_t strides[1] = {row_bytes};
   cuuint32_t box[2] = {box_inner, box_rows};

@@ -22,6 +22,16 @@ namespace tara {
 int tma_encode_tile(CUtensorMap* map, CUtensorMapDataType dt, void* base, uint64_t inner_elems,
                     uint64_t rows, uint64_t row_bytes, uint32_t box_inner, uint32_t box_rows);
 
+// A pool of nf fields back to back ([nf][Ny][ld]) as one 3D tensor; box
+// {2*CB, box_rows, 1}.
+int tma_encode_tile3(CUtensorMap* map, CUtensorMapDataType dt, void* base, uint64_t inner_elems, uint64_t rows,
+                     uint64_t nf, uint64_t row_bytes, uint64_t field_bytes, uint32_t box_inner, uint32_t box_rows);
+template <class T>
+inline int make_pool_tile_map(CUtensorMap* map, const Cx<T>* base, int ld, int Ny, int nf, int CB, int box_rows) {
+  const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  return tma_encode_tile3(map, dt, const_cast<Cx<T>*>(base), 2ull * ld, (uint64_t)Ny, (uint64_t)nf,
+                          (uint64_t)ld * sizeof(Cx<T>), (uint64_t)ld * Ny * sizeof(Cx<T>), 2u * CB, (uint32_t)box_rows);
+}
 template <class T>
 inline int make_col_tile_map(CUtensorMap* map, const Cx<T>* base, int ld, int Ny, int CB, int box_rows) {
   const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -69,6 +79,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
 // later async-proxy (TMA) accesses of the same memory.
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
 }
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
   asm volatile(
