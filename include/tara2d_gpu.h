@@ -191,6 +191,34 @@ void ab2com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const doub
              double* d_E_k_dt_old, double* d_E_k_dt_new, double* d_Bx_k_dt_old,
              double* d_Bx_k_dt_new, double* d_By_k_dt_old, double* d_By_k_dt_new);
 
+/* Incompressible vorticity models.  These take their parameters as
+ * arguments, not from COMMON.  derive2csh_/derive2css_ use the reference's
+ * pi = 3.1428 (a default-real literal), with Lx = Ly = 2 pi for csh.
+ * derive2csh_ replaces src/derive2csh.f95:3 and writes dt_omegak_new;
+ * ab2csh_ replaces src/ab2csh.f95:3 and writes omegak_new. */
+void derive2csh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* nu,
+                 const double* time, double* omegak, double* omegak_new, double* dt_omegak_old,
+                 double* dt_omegak_new);
+void ab2csh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* nu,
+             const double* time, const double* dt, double* omegak, double* omegak_new,
+             double* dt_omegak_old, double* dt_omegak_new);
+/* Screened model.  derive2css_ replaces src/derive2css.f95:6 and ab2css_
+ * replaces src/ab2css.f95:6.  rk42css_ replaces src/rk42css.f95:6, which reads
+ * uninitialised stage derivatives; here it takes one classical RK4 step and
+ * writes omegak_new only.  The reference never sets Lx, Ly and lambda in
+ * derive2css; they come from tara_set_css_box (default 2 pi, 2 pi, 10, the
+ * driver's values at src/main2css.f95:78-87). */
+void derive2css_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* alpha,
+                 const double* nu, const double* time, double* omegak, double* omegak_new,
+                 double* dt_omegak_old, double* dt_omegak_new);
+void ab2css_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* alpha,
+             const double* nu, const double* time, const double* dt, double* omegak,
+             double* omegak_new, double* dt_omegak_old, double* dt_omegak_new);
+void rk42css_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* alpha,
+              const double* nu, const double* time, const double* dt, double* omegak,
+              double* omegak_new, double* dt_omegak_old, double* dt_omegak_new);
+int tara_set_css_box(double Lx, double Ly, double lambda);
+
 /* Status of the last drop-in call of the calling thread. */
 int tara_legacy_status(void);
 /* Semantics of pc_*2coh_ / rk4_*2coh_:

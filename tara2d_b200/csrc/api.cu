@@ -783,3 +783,106 @@ void ab2com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const doub
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- vorticity
+namespace {
+// Box of derive2css, whose Lx, Ly and lambda are never set in the reference
+// (src/derive2css.f95:12, 24, 32); the driver's values (src/main2css.f95:78-87)
+// are the defaults.
+double g_css_Lx = 2.0 * 3.14159265358979323846, g_css_Ly = 2.0 * 3.14159265358979323846, g_css_lambda = 10.0;
+
+// real(kind=8), parameter :: pi = 3.1428   (a default-real literal;
+// src/derive2csh.f95:16, src/derive2css.f95:15)
+const double kVortPi = (double)3.1428f;
+
+tara_params csh_params(double nu, double dt) {
+  tara_params p{};
+  p.pi = kVortPi;
+  p.Lx = 2.0 * kVortPi;  // src/derive2csh.f95:20-21
+  p.Ly = 2.0 * kVortPi;
+  p.nu = nu;
+  p.dt = dt;
+  return p;
+}
+tara_params css_params(double alpha, double nu, double dt) {
+  tara_params p{};
+  p.pi = kVortPi;
+  p.Lx = g_css_Lx;
+  p.Ly = g_css_Ly;
+  p.lambda = g_css_lambda;
+  p.alpha = alpha;
+  p.nu = nu;
+  p.dt = dt;
+  return p;
+}
+}  // namespace
+
+extern "C" {
+
+int tara_set_css_box(double Lx, double Ly, double lambda) {
+  if (!(Lx > 0) || !(Ly > 0)) { set_error("box lengths must be positive"); return TARA_EINVAL; }
+  std::lock_guard<std::mutex> lk(g_legacy_mu);
+  g_css_Lx = Lx;
+  g_css_Ly = Ly;
+  g_css_lambda = lambda;
+  return TARA_OK;
+}
+
+void derive2csh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* nu, const double* time,
+                 double* omegak, double* omegak_new, double* dt_omegak_old, double* dt_omegak_new) {
+  (void)time; (void)omegak_new; (void)dt_omegak_old;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* in[1] = {omegak};
+  double* out[1] = {dt_omegak_new};
+  legacy_derive(TARA_MODEL_CSH, *Nx, *Ny, csh_params(*nu, 0.0), in, out);
+}
+void ab2csh_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* nu, const double* time,
+             const double* dt, double* omegak, double* omegak_new, double* dt_omegak_old, double* dt_omegak_new) {
+  (void)time;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* u[1] = {omegak};
+  const double* dn[1] = {dt_omegak_new};
+  const double* dol[1] = {dt_omegak_old};
+  double* out[1] = {omegak_new};
+  legacy_elementwise(TARA_MODEL_CSH, *Nx, *Ny, csh_params(*nu, *dt), EW_AB2, 1, u, dn, dol, out);
+}
+void derive2css_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* alpha, const double* nu,
+                 const double* time, double* omegak, double* omegak_new, double* dt_omegak_old,
+                 double* dt_omegak_new) {
+  (void)time; (void)omegak_new; (void)dt_omegak_old;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* in[1] = {omegak};
+  double* out[1] = {dt_omegak_new};
+  legacy_derive(TARA_MODEL_CSS, *Nx, *Ny, css_params(*alpha, *nu, 0.0), in, out);
+}
+void ab2css_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* alpha, const double* nu,
+             const double* time, const double* dt, double* omegak, double* omegak_new, double* dt_omegak_old,
+             double* dt_omegak_new) {
+  (void)time;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  const double* u[1] = {omegak};
+  const double* dn[1] = {dt_omegak_new};
+  const double* dol[1] = {dt_omegak_old};
+  double* out[1] = {omegak_new};
+  legacy_elementwise(TARA_MODEL_CSS, *Nx, *Ny, css_params(*alpha, *nu, *dt), EW_AB2, 1, u, dn, dol, out);
+}
+// src/rk42css.f95:6-52 reads its stage derivatives from an uninitialised
+// local; this entry point takes one classical RK4 step of derive2css instead
+// and writes omegak_new only.
+void rk42css_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nh, const double* alpha, const double* nu,
+              const double* time, const double* dt, double* omegak, double* omegak_new, double* dt_omegak_old,
+              double* dt_omegak_new) {
+  (void)time; (void)dt_omegak_old; (void)dt_omegak_new;
+  if (!check_dims(Nx, Ny, Nh)) return;
+  std::lock_guard<std::mutex> lk(g_legacy_mu);
+  int st = TARA_OK;
+  tara_session* s = legacy_session(TARA_MODEL_CSS, *Nx, *Ny, css_params(*alpha, *nu, *dt), st);
+  const double* in[1] = {omegak};
+  double* out[1] = {omegak_new};
+  if (s) st = s->set_fields(0, in);
+  if (st == TARA_OK) st = s->step(TARA_STEP_RK4, 1);
+  if (st == TARA_OK) st = s->get_fields(0, out);
+  g_legacy_status = st;
+}
+
+}  // extern "C"

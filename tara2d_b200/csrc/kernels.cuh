@@ -57,7 +57,10 @@ template <> struct RowCfg<192> { static constexpr int P = 24; };
 #define TARA_ROW_LB(tpr) ((tpr) >= 128 ? ((tpr) <= 1024 ? (tpr) : 1024) : 128)
 
 // ------------------------------------------------------------ multipliers
-enum : int { MUL_ONE = 0, MUL_IKY = 1, MUL_KY2 = 2 };
+// MUL_ONE..MUL_KY2 depend on ky only.  The streamfunction modes depend on kx
+// as well: psi = omega/(kx^2 + ky^2 + lambda), zero at k = 0, and
+// wd = (kx^2 + ky^2) psi  (src/derive2csh.f95:28-56, src/derive2css.f95:20-56).
+enum : int { MUL_ONE = 0, MUL_IKY = 1, MUL_KY2 = 2, MUL_PSI = 3, MUL_IKY_PSI = 4, MUL_WD = 5, MUL_IKY_WD = 6 };
 
 template <class T>
 __device__ __forceinline__ Cx<T> apply_ymul(int mul, T ky, Cx<T> x) {
@@ -66,12 +69,41 @@ __device__ __forceinline__ Cx<T> apply_ymul(int mul, T ky, Cx<T> x) {
   return x;
 }
 
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+// kx*kx + ky*ky rounded as written (no fused multiply-add)
+template <class T> __device__ __forceinline__ T ksq(T kx, T ky) { return mul_rn(kx, kx) + mul_rn(ky, ky); }
+
+// Streamfunction multipliers at (kx index c, ky index j); lam = 0 gives the
+// unscreened model.
+template <class T>
+__device__ __forceinline__ Cx<T> apply_psi_mul(int mul, T lam, T kx, T ky, bool origin, Cx<T> w) {
+  const T k2 = ksq(kx, ky);
+  const T den = k2 + lam;
+  const Cx<T> psi = origin ? cx<T>(0, 0) : cx<T>(w.x / den, w.y / den);
+  switch (mul) {
+    case MUL_PSI: return psi;
+    case MUL_IKY_PSI: return ikmul(ky, psi);
+    case MUL_WD: return rmul(k2, psi);
+    default: return ikmul(ky, rmul(k2, psi));  // MUL_IKY_WD
+  }
+}
+
 // ------------------------------------------------------------ inverse y pass
 template <class T> struct ColInvJob {
   const Cx<T>* src;
   Cx<T>* dst;
   int mul;
+  T lam;  // screening constant of the streamfunction modes
 };
+
+// Multiplier of job jb at (column c, row i).
+template <class T>
+__device__ __forceinline__ Cx<T> apply_job_mul(const ColInvJob<T>& jb, const Tables<T>& tb, int c, int i, Cx<T> x) {
+  const T ky = __ldg(tb.ky + i);
+  if (jb.mul < MUL_PSI) return apply_ymul(jb.mul, ky, x);
+  return apply_psi_mul(jb.mul, jb.lam, __ldg(tb.kx + c), ky, c == 0 && i == 0, x);
+}
 template <class T> struct ColInvArgs {
   Tables<T> tb;
   ColInvJob<T> job[8];
@@ -86,12 +118,11 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_inv(c
   const ColInvJob<T> jb = a.job[blockIdx.y];
   const int c0 = blockIdx.x * CB;
   const int Nh = a.tb.Nh, ld = a.tb.ld;
-  const T* ky = a.tb.ky;
   Cx<T> v[P];
   fft_run<F, +1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
     const int c = c0 + t;
     if (c >= Nh) return cx<T>(0, 0);
-    return apply_ymul(jb.mul, __ldg(ky + i), ldg(jb.src + (size_t)i * ld + c));
+    return apply_job_mul(jb, a.tb, c, i, ldg(jb.src + (size_t)i * ld + c));
   }, SyncBlock{});
   fft_emit<F>(threadIdx.x, v, [&](int t, int i, Cx<T> x) {
     const int c = c0 + t;
@@ -127,7 +158,6 @@ __global__ void __launch_bounds__(CB * L / P, 1) k_col_inv_tma(const __grid_cons
   const int tid = threadIdx.x;
   const int nitems = a.ntiles * a.njobs;
   const int Nh = a.tb.Nh, ld = a.tb.ld;
-  const T* ky = a.tb.ky;
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
@@ -164,7 +194,9 @@ __global__ void __launch_bounds__(CB * L / P, 1) k_col_inv_tma(const __grid_cons
     const int c0 = tile * CB;
     Cx<T> v[P];
     fft_run<F, +1>(sm, tid, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
-      return apply_ymul(jb.mul, __ldg(ky + i), sm[i * CB + t]);
+      // columns past Nh hold the TMA fill value (zero); keep kx in range
+      const int c = c0 + t < Nh ? c0 + t : Nh - 1;
+      return apply_job_mul(jb, a.tb, c, i, sm[i * CB + t]);
     }, SyncBlock{});
     fft_emit<F>(tid, v, [&](int t, int i, Cx<T> x) {
       const int c = c0 + t;
