@@ -95,6 +95,24 @@ int tara_synchronize(tara_session* s);
 int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms);
 /* Kernel launches one step of the given stepper issues. */
 int tara_launches_per_step(const tara_session* s, int stepper);
+
+/* ---- diagnostics, computed on the device from the resident state ----
+ * Values (all sums in FP64 whatever the precision; the last two are 0):
+ *   MHD   (src/main2com.f95:587-604, the Energy.dat line after `time`):
+ *         Energy = <|u|^2>, B_Field = <|B|^2>, C2 = <omega^2>, C3 = <j^2>,
+ *         div_B_Tot = <div B>, then the cross-helicity <u.B>
+ *   hydro (src/main2coh.f95:321-429): Energy/2, y_Energy/2, C0, C1, C2, C3
+ *         (C_n = <omega^n>)
+ * E(k): tara_num_shells() shells, E(k) = sum over floor(|k| + 1/2) = k of
+ * (|ux_k|^2 + |uy_k|^2)/2/(NxNy)^2 (modes 0 < kx index < Nx/2 counted twice).
+ * Vorticity models: TARA_EUNSUPPORTED. */
+#define TARA_DIAG_VALUES 8
+int tara_num_shells(tara_session* s);
+int tara_diagnostics(tara_session* s, double* out, int nout, double* Ek, int nbins);
+/* nrec records of TARA_DIAG_VALUES + tara_num_shells() doubles: the first of
+ * the current state, then one after every `every` steps (nsteps = (nrec - 1)
+ * * every in all).  Records stay on the device until the run ends. */
+int tara_run_recorded(tara_session* s, int stepper, int every, int nrec, double* rec);
 /* Advance nsteps with a CUDA event recorded before every kernel; returns, per
  * kernel kind (index 0..TARA_NUM_KERNEL_KINDS-1, see tara_kernel_name), the
  * summed device time in ms and the number of launches, plus the total. */

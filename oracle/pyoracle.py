@@ -67,6 +67,10 @@ def lib():
         L.ora_run_com.argtypes = [i, i, d, C.POINTER(ComParams), i, i, P, P]
         L.ora_diag_com.argtypes = [i, i, d, C.POINTER(ComParams), P, P]
         L.ora_diag_coh.argtypes = [i, i, d, C.POINTER(CohParams), P, P, P, P]
+        L.ora_num_shells.argtypes = [i, i, d, d, d]
+        L.ora_num_shells.restype = i
+        L.ora_spectrum_coh.argtypes = [i, i, d, C.POINTER(CohParams), P, P, i, P]
+        L.ora_spectrum_com.argtypes = [i, i, d, C.POINTER(ComParams), P, i, P]
         L.ora_set_threads.argtypes = [i]
         L.ora_get_threads.restype = i
     return _lib
@@ -243,4 +247,24 @@ def diag_coh(Nx, Ny, P: CohParams, state, pi=PI):
     st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
     out = np.zeros(6)
     lib().ora_diag_coh(Nx, Ny, pi, C.byref(P), *[_p(a) for a in st], _p(out))
+    return out
+
+
+def num_shells(Nx, Ny, Lx=2 * PI, Ly=2 * PI, pi=PI):
+    return lib().ora_num_shells(Nx, Ny, pi, Lx, Ly)
+
+
+def spectrum_coh(Nx, Ny, P: CohParams, ukx, uky, pi=PI):
+    n = num_shells(Nx, Ny, P.Lx, P.Ly, pi)
+    a = [np.ascontiguousarray(x, dtype=np.complex128) for x in (ukx, uky)]
+    out = np.zeros(n)
+    lib().ora_spectrum_coh(Nx, Ny, pi, C.byref(P), _p(a[0]), _p(a[1]), n, _p(out))
+    return out
+
+
+def spectrum_com(Nx, Ny, P: ComParams, state, pi=PI):
+    n = num_shells(Nx, Ny, P.Lx, P.Ly, pi)
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    out = np.zeros(n)
+    lib().ora_spectrum_com(Nx, Ny, pi, C.byref(P), _ptr_array(st), n, _p(out))
     return out

@@ -783,3 +783,57 @@ void ora_diag_coh(int Nx, int Ny, double pi, const ora_coh_params *P,
   out[2] = C0 / NN; out[3] = C1 / NN; out[4] = C2 / NN; out[5] = C3 / NN;
   fftw_free(omk); fftw_free(ux); fftw_free(uy); fftw_free(om); fftw_free(n);
 }
+
+/* ---- shell spectrum E(k) (a definition of this build; the reference keeps
+ * only a commented-out per-mode listing at src/main2com.f95:566-577) ----
+ * E(k) = sum over floor(|k| + 1/2) = k of (|ux_k|^2 + |uy_k|^2) / 2 / (NxNy)^2,
+ * half-spectrum modes with 0 < i < Nx/2 counted twice.  Velocity spectra are
+ * the unnormalised forward transforms of the velocity. */
+int ora_num_shells(int Nx, int Ny, double pi, double Lx, double Ly) {
+  const double kxm = kx_of(Nx / 2, pi, Lx), kym = fabs(ky_of(Ny / 2, Ny, pi, Ly));
+  return (int)floor(sqrt(kxm * kxm + kym * kym) + 0.5) + 1;
+}
+
+static void shell_spectrum(int Nx, int Ny, double pi, double Lx, double Ly, const ocplx *uxk,
+                           const ocplx *uyk, int nbins, double *Ek) {
+  const int Nh = Nx / 2 + 1;
+  const double NN = (double)Nx * (double)Ny;
+  for (int s = 0; s < nbins; s++) Ek[s] = 0.0;
+  for (int j = 0; j < Ny; j++)
+    for (int i = 0; i < Nh; i++) {
+      const double kx = kx_of(i, pi, Lx), ky = ky_of(j, Ny, pi, Ly);
+      const int s = (int)floor(sqrt(kx * kx + ky * ky) + 0.5);
+      const size_t k = IX(i, j, Nh);
+      const double w = (i > 0 && i < Nx / 2) ? 2.0 : 1.0;
+      const double e = creal(uxk[k]) * creal(uxk[k]) + cimag(uxk[k]) * cimag(uxk[k]) +
+                       creal(uyk[k]) * creal(uyk[k]) + cimag(uyk[k]) * cimag(uyk[k]);
+      if (s < nbins) Ek[s] += 0.5 * w * e;
+    }
+  for (int s = 0; s < nbins; s++) Ek[s] = Ek[s] / NN / NN;
+}
+
+void ora_spectrum_coh(int Nx, int Ny, double pi, const ora_coh_params *P, const ocplx *ukx, const ocplx *uky,
+                      int nbins, double *Ek) {
+  shell_spectrum(Nx, Ny, pi, P->Lx, P->Ly, ukx, uky, nbins, Ek);
+}
+
+/* velocity of the MHD state as in src/main2com.f95:446-480: u = c2r(rho u)/c2r(rho) */
+void ora_spectrum_com(int Nx, int Ny, double pi, const ora_com_params *P, const ocplx *const state[6], int nbins,
+                      double *Ek) {
+  const int Nh = Nx / 2 + 1;
+  const double NN = (double)Nx * (double)Ny;
+  double *rho = rnew(Nx, Ny), *ux = rnew(Nx, Ny), *uy = rnew(Nx, Ny);
+  ocplx *uxk = cnew(Nh, Ny), *uyk = cnew(Nh, Ny);
+  ora_c2r_2d(Nx, Ny, state[0], rho);
+  ora_c2r_2d(Nx, Ny, state[1], ux);
+  ora_c2r_2d(Nx, Ny, state[2], uy);
+  for (size_t k = 0; k < (size_t)Nx * Ny; k++) {
+    rho[k] /= NN;
+    ux[k] = (ux[k] / NN) / rho[k];
+    uy[k] = (uy[k] / NN) / rho[k];
+  }
+  ora_r2c_2d(Nx, Ny, ux, uxk);
+  ora_r2c_2d(Nx, Ny, uy, uyk);
+  shell_spectrum(Nx, Ny, pi, P->Lx, P->Ly, uxk, uyk, nbins, Ek);
+  fftw_free(rho); fftw_free(ux); fftw_free(uy); fftw_free(uxk); fftw_free(uyk);
+}

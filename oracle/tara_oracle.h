@@ -119,6 +119,15 @@ void ora_diag_com(int Nx, int Ny, double pi, const ora_com_params *P, const ocpl
 void ora_diag_coh(int Nx, int Ny, double pi, const ora_coh_params *P,
                   const ocplx *nk, const ocplx *ukx, const ocplx *uky, double out[6]);
 
+/* ---- shell spectrum E(k) = sum_{floor(|k|+1/2)=k} (|ux_k|^2+|uy_k|^2)/2/(NxNy)^2 ----
+ * (not in the reference, which only lists modes in commented-out code at
+ * src/main2com.f95:566-577); nbins from ora_num_shells. */
+int ora_num_shells(int Nx, int Ny, double pi, double Lx, double Ly);
+void ora_spectrum_coh(int Nx, int Ny, double pi, const ora_coh_params *P, const ocplx *ukx, const ocplx *uky,
+                      int nbins, double *Ek);
+void ora_spectrum_com(int Nx, int Ny, double pi, const ora_com_params *P, const ocplx *const state[6], int nbins,
+                      double *Ek);
+
 /* number of OpenMP threads the pointwise loops use (0 = runtime default) */
 void ora_set_threads(int n);
 int  ora_get_threads(void);

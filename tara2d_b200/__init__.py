@@ -27,8 +27,12 @@ STEP_AB2, STEP_RK4, STEP_EULER = 0, 1, 2
 LEGACY_REFERENCE, LEGACY_CORRECT = 0, 1
 SUPPORTED_N = (16, 32, 64, 128, 256, 384, 512, 1024, 2048, 4096)
 NUM_KERNEL_KINDS = 11
+DIAG_VALUES = 8
 NFIELDS = {MODEL_COH: 3, MODEL_COM: 6, MODEL_CSH: 1, MODEL_CSS: 1}
 PI = 3.14159265358979323846
+# pi of the vorticity subroutines: real(kind=8), parameter :: pi = 3.1428, a
+# default-real literal (src/derive2csh.f95:16, src/derive2css.f95:15)
+VORT_PI = float(np.float32(3.1428))
 
 
 class TaraError(RuntimeError):
@@ -86,6 +90,10 @@ def lib():
         L.tara_host_unregister.argtypes = [P]
         L.tara_device_pci_bus_id.argtypes = [C.c_char_p, I]
         L.tara_set_device.argtypes = [I]
+        L.tara_num_shells.argtypes = [P]
+        L.tara_diagnostics.argtypes = [P, P, I, P, I]
+        L.tara_run_recorded.argtypes = [P, I, I, I, P]
+        L.tara_set_css_box.argtypes = [D, D, D]
         _lib = L
     return _lib
 
@@ -185,6 +193,25 @@ class Session:
 
     def launches_per_step(self, stepper: int) -> int:
         return lib().tara_launches_per_step(self._h, stepper)
+
+    def num_shells(self) -> int:
+        return lib().tara_num_shells(self._h)
+
+    def diagnostics(self):
+        """(values[DIAG_VALUES], E(k)[num_shells]) of the current state, computed on the device."""
+        out = np.zeros(DIAG_VALUES)
+        ek = np.zeros(self.num_shells())
+        check(lib().tara_diagnostics(self._h, out.ctypes.data, DIAG_VALUES, ek.ctypes.data, ek.size),
+              "tara_diagnostics")
+        return out, ek
+
+    def run_recorded(self, stepper: int, every: int, nrec: int):
+        """Records of the state before the first step and after every `every`
+        steps: (values[nrec, DIAG_VALUES], E(k)[nrec, num_shells])."""
+        ns = self.num_shells()
+        rec = np.zeros((nrec, DIAG_VALUES + ns))
+        check(lib().tara_run_recorded(self._h, stepper, every, nrec, rec.ctypes.data), "tara_run_recorded")
+        return rec[:, :DIAG_VALUES], rec[:, DIAG_VALUES:]
 
     def profile_steps(self, stepper: int, nsteps: int):
         """Per-kernel device time: {name: (total_ms, launches)} and the total ms."""

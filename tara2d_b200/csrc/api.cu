@@ -6,7 +6,9 @@
 #include <memory>
 #include <mutex>
 #include <tuple>
+#include <vector>
 #include "models.h"
+#include "diag.cuh"
 
 using namespace tara;
 
@@ -117,6 +119,11 @@ struct tara_session {
   // per-field PC / RK4 with the other hydro fields frozen (TARA_LEGACY_CORRECT)
   virtual int frozen_field_step(bool rk4, int which, const double* const* f, const double* d,
                                 double* out) = 0;
+  virtual int num_shells() = 0;
+  // nrec diagnostics records of the state, one before the first step and one
+  // after every `every` steps (nsteps = (nrec - 1) * every), into rec
+  // (host, nrec * (TARA_DIAG_VALUES + num_shells()) doubles)
+  virtual int run_recorded(int stepper, int every, int nrec, double* rec) = 0;
 };
 
 namespace {
@@ -132,11 +139,12 @@ struct SessionT : tara_session {
   CohParamsT<T> cohp{};
   ComParamsT<T> comp{};
   VortParamsT<T> vortp{};
+  DiagWork<T> dw;
 
   ~SessionT() override {
     if (st) cudaStreamSynchronize(st);
     g.release(); u.release(); unew.release(); dold.release(); acc.release(); us.release(); us2.release();
-    tmp.release();
+    tmp.release(); dw.release();
     stage.release(); cw.release(); mw.release(); vw.release();
   }
 
@@ -377,6 +385,43 @@ struct SessionT : tara_session {
     int per = model == TARA_MODEL_COH ? kCohLaunches : model == TARA_MODEL_COM ? kComLaunches : kVortLaunches;
     return stepper == TARA_STEP_RK4 ? 4 * per : per;
   }
+
+  int num_shells() override { return diag_num_shells(Nx, Ny, p.Lx, p.Ly, p.pi); }
+  int record(double* drec) {
+    if (!dw.mem || dw.nbins != num_shells()) {
+      dw.release();
+      TARA_TRY(dw.alloc(g, st));
+    }
+    Cx<T>* state[6];
+    for (int f = 0; f < nf; f++) state[f] = u[f];
+    if (model == TARA_MODEL_COM) return diag_record(model, g, dw, state, mw.H, mw.X, tmp, drec, st);
+    return diag_record(model, g, dw, state, cw.H, cw.X, tmp, drec, st);
+  }
+  int run_recorded(int stepper, int every, int nrec, double* rec) override {
+    if (!rec || nrec < 1 || every < 0 || (nrec > 1 && every < 1)) { set_error("bad record request"); return TARA_EINVAL; }
+    if (model != TARA_MODEL_COM && model != TARA_MODEL_COH) {
+      set_error("diagnostics are defined for the hydro and MHD models");
+      return TARA_EUNSUPPORTED;
+    }
+    const size_t per = (size_t)kDiagOut + (size_t)num_shells();
+    double* d = nullptr;
+    if (cudaMalloc(&d, per * nrec * sizeof(double)) != cudaSuccess) {
+      set_error("cudaMalloc of the diagnostics records failed");
+      return TARA_ENOMEM;
+    }
+    int r = TARA_OK;
+    for (int k = 0; k < nrec && r == TARA_OK; k++) {
+      if (k > 0) r = step(stepper, every);
+      if (r == TARA_OK) r = record(d + per * k);
+    }
+    if (r == TARA_OK && cudaMemcpyAsync(rec, d, per * nrec * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      r = TARA_ECUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess && r == TARA_OK) r = TARA_ECUDA;
+    if (r == TARA_ECUDA) set_error(std::string("diagnostics: ") + cudaGetErrorString(cudaGetLastError()));
+    cudaFree(d);
+    if (r != TARA_OK) return r;
+    return device_status();
+  }
 };
 
 tara_session* make_session(int precision) {
@@ -550,6 +595,27 @@ int tara_device_pci_bus_id(char* out, int len) {
 }
 
 int tara_launches_per_step(const tara_session* s, int stepper) { return s ? s->launches(stepper) : 0; }
+
+int tara_num_shells(tara_session* s) { return s ? s->num_shells() : 0; }
+int tara_diagnostics(tara_session* s, double* out, int nout, double* Ek, int nbins) {
+  if (!s || (!out && nout > 0) || (!Ek && nbins > 0) || nout < 0 || nbins < 0) return TARA_EINVAL;
+  const int ns = s->num_shells();
+  if (nout > TARA_DIAG_VALUES || nbins > ns) { set_error("more values requested than computed"); return TARA_EINVAL; }
+  std::vector<double> rec((size_t)TARA_DIAG_VALUES + ns);
+  int r = s->run_recorded(TARA_STEP_RK4, 0, 1, rec.data());
+  if (r != TARA_OK) return s->fail_if(r);
+  for (int k = 0; k < nout; k++) out[k] = rec[k];
+  for (int k = 0; k < nbins; k++) Ek[k] = rec[TARA_DIAG_VALUES + k];
+  return TARA_OK;
+}
+int tara_run_recorded(tara_session* s, int stepper, int every, int nrec, double* rec) {
+  if (!s) return TARA_EINVAL;
+  if (stepper != TARA_STEP_AB2 && stepper != TARA_STEP_EULER && stepper != TARA_STEP_RK4) {
+    set_error("unknown stepper");
+    return TARA_EINVAL;
+  }
+  return s->fail_if(s->run_recorded(stepper, every, nrec, rec));
+}
 int tara_status(const tara_session* s) { return s ? s->status : TARA_EINVAL; }
 
 }  // extern "C"

@@ -278,6 +278,7 @@ template <class T> struct ColFwdSimpleArgs {
   Tables<T> tb;
   const Cx<T>* X[6];
   T sign[6];  // derivative = sign * dealiased transform
+  int nomask;  // 1: plain forward transform (no dealiasing)
   StepArgs<T> step;
 };
 
@@ -300,7 +301,7 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_s
   fft_emit<F>(threadIdx.x, v, [&](int t, int j, Cx<T> x) {
     const int c = c0 + t;
     if (c >= Nh) return;
-    const bool masked = c >= __ldg(a.tb.cut + j);
+    const bool masked = !a.nomask && c >= __ldg(a.tb.cut + j);
     Cx<T> val = masked ? cx<T>(0, 0) : x;
     Cx<T> d = cx<T>(sg * val.x, sg * val.y);
     step_apply(a.step, f, (size_t)j * ld + c, d);
