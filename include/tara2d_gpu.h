@@ -95,6 +95,10 @@ int tara_synchronize(tara_session* s);
 int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms);
 /* Kernel launches one step of the given stepper issues. */
 int tara_launches_per_step(const tara_session* s, int stepper);
+/* Steps are replayed from CUDA graphs of two steps each (captured on first
+ * use per stepper, dropped on tara_set_params); on = 0 launches every kernel
+ * from the host instead.  Default: on. */
+int tara_set_graphs(tara_session* s, int on);
 
 /* ---- diagnostics, computed on the device from the resident state ----
  * Values (all sums in FP64 whatever the precision; the last two are 0):

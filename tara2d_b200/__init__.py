@@ -90,6 +90,7 @@ def lib():
         L.tara_host_unregister.argtypes = [P]
         L.tara_device_pci_bus_id.argtypes = [C.c_char_p, I]
         L.tara_set_device.argtypes = [I]
+        L.tara_set_graphs.argtypes = [P, I]
         L.tara_num_shells.argtypes = [P]
         L.tara_diagnostics.argtypes = [P, P, I, P, I]
         L.tara_run_recorded.argtypes = [P, I, I, I, P]
@@ -193,6 +194,10 @@ class Session:
 
     def launches_per_step(self, stepper: int) -> int:
         return lib().tara_launches_per_step(self._h, stepper)
+
+    def set_graphs(self, on: bool) -> None:
+        """Replay steps from CUDA graphs (default) or launch every kernel from the host."""
+        check(lib().tara_set_graphs(self._h, 1 if on else 0), "tara_set_graphs")
 
     def num_shells(self) -> int:
         return lib().tara_num_shells(self._h)

@@ -120,6 +120,7 @@ struct tara_session {
   virtual int frozen_field_step(bool rk4, int which, const double* const* f, const double* d,
                                 double* out) = 0;
   virtual int num_shells() = 0;
+  virtual void set_graphs(bool on) = 0;
   // nrec diagnostics records of the state, one before the first step and one
   // after every `every` steps (nsteps = (nrec - 1) * every), into rec
   // (host, nrec * (TARA_DIAG_VALUES + num_shells()) doubles)
@@ -143,6 +144,7 @@ struct SessionT : tara_session {
 
   ~SessionT() override {
     if (st) cudaStreamSynchronize(st);
+    drop_graphs();
     g.release(); u.release(); unew.release(); dold.release(); acc.release(); us.release(); us2.release();
     tmp.release(); dw.release();
     stage.release(); cw.release(); mw.release(); vw.release();
@@ -179,6 +181,7 @@ struct SessionT : tara_session {
   }
 
   int apply_params() override {
+    drop_graphs();
     if (p.Lx != g.Lx || p.Ly != g.Ly || p.pi != g.pi) {
       // wavenumber tables depend on Lx, Ly and pi
       TARA_CUDA_TRY(cudaStreamSynchronize(st));
@@ -293,11 +296,69 @@ struct SessionT : tara_session {
   // (the RHS of one field reads other fields of its input state, so no
   // kernel may update a state it also reads); the two are swapped after the
   // step.  RK4 stage inputs alternate between us and us2 for the same reason.
+  // CUDA graphs of two steps (after which u and unew are back in place), one
+  // per (stepper, buffer holding the state); kernel arguments are baked in,
+  // so a parameter change drops them.
+  struct StepGraph {
+    int stepper = -1;
+    const void* ubase = nullptr;
+    cudaGraphExec_t exec = nullptr;
+  };
+  StepGraph graphs[6];
+  void drop_graphs() {
+    for (auto& gr : graphs) {
+      if (gr.exec) cudaGraphExecDestroy(gr.exec);
+      gr = StepGraph{};
+    }
+  }
+  cudaGraphExec_t pair_graph(int stepper) {
+    for (auto& gr : graphs)
+      if (gr.exec && gr.stepper == stepper && gr.ubase == u.base) return gr.exec;
+    StepGraph* slot = nullptr;
+    for (auto& gr : graphs)
+      if (!gr.exec) { slot = &gr; break; }
+    if (!slot) { drop_graphs(); slot = &graphs[0]; }
+    const void* ub = u.base;
+    const FieldPool<T> u0 = u, unew0 = unew;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return nullptr;
+    int r = launch_steps(stepper, 2);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    u = u0;  // nothing ran while capturing
+    unew = unew0;
+    cudaGetLastError();
+    cudaGraphExec_t exec = nullptr;
+    if (r == TARA_OK && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) exec = nullptr;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (!exec) return nullptr;
+    slot->stepper = stepper;
+    slot->ubase = ub;
+    slot->exec = exec;
+    return exec;
+  }
+  bool use_graphs = true;
+  void set_graphs(bool on) override {
+    use_graphs = on;
+    if (!on) drop_graphs();
+  }
+
   int step(int stepper, int n) override {
     if (stepper != TARA_STEP_AB2 && stepper != TARA_STEP_EULER && stepper != TARA_STEP_RK4) {
       set_error("unknown stepper");
       return TARA_EINVAL;
     }
+    int done = 0;
+    if (use_graphs && !prof.on && n >= 2) {
+      cudaGraphExec_t ex = pair_graph(stepper);
+      if (ex) {
+        // capture swapped u/unew twice: the state is back in the same buffer
+        for (; done + 2 <= n; done += 2) TARA_CUDA_TRY(cudaGraphLaunch(ex, st));
+      }
+    }
+    return launch_steps(stepper, n - done);
+  }
+  int launch_steps(int stepper, int n) {
     for (int t = 0; t < n; t++) {
       Cx<T>* in_u[6];
       for (int f = 0; f < nf; f++) in_u[f] = u[f];
@@ -596,6 +657,11 @@ int tara_device_pci_bus_id(char* out, int len) {
 
 int tara_launches_per_step(const tara_session* s, int stepper) { return s ? s->launches(stepper) : 0; }
 
+int tara_set_graphs(tara_session* s, int on) {
+  if (!s) return TARA_EINVAL;
+  s->set_graphs(on != 0);
+  return TARA_OK;
+}
 int tara_num_shells(tara_session* s) { return s ? s->num_shells() : 0; }
 int tara_diagnostics(tara_session* s, double* out, int nout, double* Ek, int nbins) {
   if (!s || (!out && nout > 0) || (!Ek && nbins > 0) || nout < 0 || nbins < 0) return TARA_EINVAL;
