@@ -43,6 +43,9 @@ inline int row_cta_rows(int threads_per_row, size_t smem_per_row, int Ny, int ma
 // (each group's output array is also its exchange buffer), phase 2 forms the
 // velocity, phase 3 runs the eight r2c in eight groups; once every group has
 // gathered its inputs the eight field arrays become their exchange buffers.
+// LOW (rows too long for eight arrays in shared memory): six arrays, the
+// velocity is formed where it is used, and the last two r2c run after the
+// first six have released their arrays.
 template <class T> struct RowCom1Args {
   Tables<T> tb;
   const Cx<T>* H[6];
@@ -51,18 +54,18 @@ template <class T> struct RowCom1Args {
   int rb;
 };
 
-template <class T, int M, int P>
+template <class T, int M, int P, bool LOW>
 __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const RowCom1Args<T> a) {
   using RF = RowFFT<M, P>;
-  constexpr int NTR = M / P, G = 8, ARR = RF::SMEM_ELEMS;
+  constexpr int NTR = M / P, G = 8, ARR = RF::SMEM_ELEMS, NA = LOW ? 6 : 8;
   extern __shared__ __align__(16) unsigned char smraw[];
   const RowThread<NTR, G> th;
   const auto sync = th.sync();
   const Tables<T>& tb = a.tb;
-  Cx<T>* base = reinterpret_cast<Cx<T>*>(smraw) + (size_t)th.row * G * ARR;
+  Cx<T>* base = reinterpret_cast<Cx<T>*>(smraw) + (size_t)th.row * NA * ARR;
   Cx<T>* f[8];  // rho, rho ux, rho uy, E, Bx, By, ux, uy (pairs x[2m], x[2m+1])
 #pragma unroll
-  for (int q = 0; q < 8; q++) f[q] = base + q * ARR;
+  for (int q = 0; q < 8; q++) f[q] = base + (q < NA ? q : q - NA) * ARR;
   const int y = blockIdx.x * a.rb + th.row;
   const size_t ro = (size_t)y * tb.ld;
   Cx<T> v[P];
@@ -78,19 +81,21 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
   }
   __syncthreads();
   // phase 2: velocity                            (:105-106)
-  for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
-    const Cx<T> rho = f[0][n], mx = f[1][n], my = f[2][n];
-    f[6][n] = cx<T>(mx.x / rho.x, mx.y / rho.y);
-    f[7][n] = cx<T>(my.x / rho.x, my.y / rho.y);
+  if constexpr (!LOW) {
+    for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
+      const Cx<T> rho = f[0][n], mx = f[1][n], my = f[2][n];
+      f[6][n] = cx<T>(mx.x / rho.x, mx.y / rho.y);
+      f[7][n] = cx<T>(my.x / rho.x, my.y / rho.y);
+    }
+    __syncthreads();
   }
-  __syncthreads();
   // phase 3: fluxes of output th.g at the stage-0 points, then r2c     (:193-213)
   const T cs2 = a.cs2;
   const int q = th.g;
   row_r2c_begin<RF>(th.lane, v, tb, [&](int n) -> Cx<T> {
     Cx<T> F[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) F[k] = f[k][n];
+    for (int k = 0; k < NA; k++) F[k] = f[k][n];
     T o[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -100,8 +105,14 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
       const T E = h ? F[3].y : F[3].x;
       const T bx = h ? F[4].y : F[4].x;
       const T by = h ? F[5].y : F[5].x;
-      const T ux = h ? F[6].y : F[6].x;
-      const T uy = h ? F[7].y : F[7].x;
+      T ux, uy;
+      if constexpr (LOW) {
+        ux = mx / rho;
+        uy = my / rho;
+      } else {
+        ux = h ? F[6].y : F[6].x;
+        uy = h ? F[7].y : F[7].x;
+      }
       const T B2 = bx * bx + by * by;
       const T Pr = cs2 * rho;
       T r;
@@ -121,7 +132,11 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
   });
   __syncthreads();  // every group has its inputs: the field arrays are free
   Cx<T>* xo = a.X[q] + ro;
-  row_r2c_finish<RF>(f[q], th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
+  if (q < NA) row_r2c_finish<RF>(f[q], th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
+  if constexpr (LOW) {
+    __syncthreads();  // arrays 0 and 1 are free again
+    if (q >= NA) row_r2c_finish<RF>(f[q], th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
+  }
 }
 
 // Forcing (only when A != 0):  Fx = -rho A sin(kf y_j), Fy = rho A sin(kf x_i)
@@ -382,9 +397,10 @@ static void launch_row_com1(const RowCom1Args<T>& a0, int Ny, cudaStream_t st) {
   constexpr int P = RowCfg<M>::P;
   constexpr int NTR = M / P;
   RowCom1Args<T> a = a0;
-  const size_t per_row = (size_t)8 * RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<T>);
+  constexpr bool LOW = (size_t)8 * RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<T>) > 200 * 1024;
+  const size_t per_row = (size_t)(LOW ? 6 : 8) * RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<T>);
   a.rb = row_cta_rows(8 * NTR, per_row, Ny);
-  auto kern = k_row_com1<T, M, P>;
+  auto kern = k_row_com1<T, M, P, LOW>;
   const size_t smem = per_row * a.rb;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<Ny / a.rb, 8 * NTR * a.rb, smem, st>>>(a);
@@ -425,7 +441,7 @@ static void launch_row_com2(const RowCom2Args<T>& a, int Ny, int fix, cudaStream
 template <class T>
 int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* const in[6],
             const StepArgs<T>& step, cudaStream_t st) {
-  if ((size_t)8 * (g.Nx / 2 + g.Nx / 32 + 1) * sizeof(Cx<T>) > 227 * 1024 || 8 * (g.Nx / 2) / 16 > 1024) {
+  if ((size_t)6 * (g.Nx / 2 + g.Nx / 32 + 1) * sizeof(Cx<T>) > 220 * 1024 || 8 * (g.Nx / 2) / 16 > 1024) {
     set_error("MHD row pass does not fit in shared memory at this Nx and precision");
     return TARA_EUNSUPPORTED;
   }

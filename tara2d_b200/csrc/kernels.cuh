@@ -27,7 +27,7 @@ template <int L> struct ColFwdComCfg<double, L> {
 };
 template <int L> struct ColFwdComCfg<float, L> {
   static constexpr int P = (L == 384) ? 24 : (L >= 512 ? 8 : 16);
-  static constexpr int CB = (L <= 256) ? 8 : 4;
+  static constexpr int CB = (L <= 256) ? 8 : (L >= 4096 ? 2 : 4);
 };
 // Row pass: P values per thread (M = Nx/2 points per row FFT).
 template <int M> struct RowCfg { static constexpr int P = 16; };
@@ -143,7 +143,9 @@ template <class T> struct ColInvTmaArgs {
 template <int L, int CB, int P> struct ColTmaLayout {
   using F = FFTB<L, CB, P>;
   static constexpr int BOX = L <= 256 ? L : (L % 256 == 0 ? 256 : 128);  // rows per TMA box (divides L)
-  static constexpr int BUFE = (F::SMEM_ELEMS + 7) / 8 * 8;  // complex elements per buffer (128-byte multiple)
+  // complex elements per buffer: a multiple of 16, so that every buffer starts
+  // on the 128-byte boundary a TMA destination needs, for 8- and 16-byte elements
+  static constexpr int BUFE = (F::SMEM_ELEMS + 15) / 16 * 16;
   template <class T> static constexpr size_t bytes() { return 2 * (size_t)BUFE * sizeof(Cx<T>) + 64; }
 };
 
@@ -343,7 +345,9 @@ inline void col_inv_dispatch(const ColInvArgs<T>& a, int njobs, cudaStream_t st)
   t.tb = a.tb;
   t.njobs = njobs;
   t.ntiles = (a.tb.Nh + CB - 1) / CB;
-  bool maps_ok = (a.tb.ld * sizeof(Cx<T>)) % 16 == 0 && (2 * CB * sizeof(T)) % 16 == 0;
+  // two column tiles must fit in shared memory (not so for the longest columns)
+  constexpr bool fits = LY::template bytes<T>() <= 220 * 1024;
+  bool maps_ok = fits && (a.tb.ld * sizeof(Cx<T>)) % 16 == 0 && (2 * CB * sizeof(T)) % 16 == 0;
   for (int q = 0; q < njobs && maps_ok; q++) {
     t.job[q] = a.job[q];
     maps_ok = make_col_tile_map<T>(&t.map[q], a.job[q].src, a.tb.ld, a.tb.Ny, CB, LY::BOX) == TARA_OK;
