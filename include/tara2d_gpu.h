@@ -117,6 +117,36 @@ int tara_diagnostics(tara_session* s, double* out, int nout, double* Ek, int nbi
  * the current state, then one after every `every` steps (nsteps = (nrec - 1)
  * * every in all).  Records stay on the device until the run ends. */
 int tara_run_recorded(tara_session* s, int stepper, int every, int nrec, double* rec);
+
+/* ---- batched ensembles (no counterpart in the reference, whose drivers run
+ * one grid per process) ----
+ * n independent hydro (*2coh) runs, member m on an N[m] x N[m] grid
+ * (N in {128, 256, 384, 512}) with its own parameters params[m] (mux, muy,
+ * CS, dt; members of one grid size share Lx, Ly, pi), advanced together: each
+ * step is three persistent launches over every member (column inverse, row
+ * pass, column forward with the AB2/Euler update), replayed from a CUDA graph.
+ * State arrays are complex(8) (Nh,Ny) host arrays as for sessions; AB2
+ * history starts at zero.  FP32 or FP64 fields; diagnostics sum in FP64. */
+typedef struct tara_ensemble tara_ensemble;
+int tara_ens_open(tara_ensemble** out, int model, int n, const int* N, const tara_params* params, int precision);
+int tara_ens_close(tara_ensemble* e);
+int tara_ens_size(const tara_ensemble* e);
+int tara_ens_set_state(tara_ensemble* e, int member, const double* const* fields3);
+int tara_ens_get_state(tara_ensemble* e, int member, double* const* fields3);
+int tara_ens_get_history(tara_ensemble* e, int member, double* const* fields3);
+int tara_ens_step(tara_ensemble* e, int stepper, int nsteps); /* TARA_STEP_AB2 or TARA_STEP_EULER */
+int tara_ens_time_steps(tara_ensemble* e, int stepper, int nsteps, float* ms);
+/* Tuning: {values per thread of the column inverse, the row pass and the
+ * column forward pass (8 or 16), CTAs per SM of each persistent grid (0 = as
+ * many as fit)}.  Default {16, 16, 16, 0, 0, 0}. */
+int tara_ens_set_tuning(tara_ensemble* e, const int* tuning6);
+int tara_ens_get_tuning(const tara_ensemble* e, int* tuning6);
+/* Times every candidate per phase on this ensemble (reps steps each, state
+ * and history restored afterwards) and keeps the fastest; chosen6 and
+ * best_ms3 (ms per step of each phase) may be NULL. */
+int tara_ens_autotune(tara_ensemble* e, int stepper, int reps, int* chosen6, float* best_ms3);
+int tara_ens_num_shells(tara_ensemble* e, int member);
+int tara_ens_diagnostics(tara_ensemble* e, int member, double* out, int nout, double* Ek, int nbins);
 /* Advance nsteps with a CUDA event recorded before every kernel; returns, per
  * kernel kind (index 0..TARA_NUM_KERNEL_KINDS-1, see tara_kernel_name), the
  * summed device time in ms and the number of launches, plus the total. */

@@ -91,6 +91,18 @@ def lib():
         L.tara_device_pci_bus_id.argtypes = [C.c_char_p, I]
         L.tara_set_device.argtypes = [I]
         L.tara_set_graphs.argtypes = [P, I]
+        L.tara_ens_open.argtypes = [C.POINTER(C.c_void_p), I, I, P, C.POINTER(Params), I]
+        L.tara_ens_close.argtypes = [P]
+        for n in ("tara_ens_set_state", "tara_ens_get_state", "tara_ens_get_history"):
+            getattr(L, n).argtypes = [P, I, PP]
+        L.tara_ens_step.argtypes = [P, I, I]
+        L.tara_ens_time_steps.argtypes = [P, I, I, C.POINTER(C.c_float)]
+        L.tara_ens_set_tuning.argtypes = [P, P]
+        L.tara_ens_get_tuning.argtypes = [P, P]
+        L.tara_ens_autotune.argtypes = [P, I, I, P, P]
+        L.tara_ens_num_shells.argtypes = [P, I]
+        L.tara_ens_diagnostics.argtypes = [P, I, P, I, P, I]
+        L.tara_ens_size.argtypes = [P]
         L.tara_num_shells.argtypes = [P]
         L.tara_diagnostics.argtypes = [P, P, I, P, I]
         L.tara_run_recorded.argtypes = [P, I, I, I, P]
@@ -262,6 +274,98 @@ def _i32(v):
 
 def _d(v):
     return C.byref(C.c_double(v))
+
+
+class Ensemble:
+    """Independent hydro runs of mixed grid sizes advanced together
+    (tara_ens_open ... tara_ens_close).  sizes[m] in {128, 256, 384, 512};
+    params[m] is a Params (or one Params for every member)."""
+
+    def __init__(self, sizes, params, precision: int = FP32, model: int = MODEL_COH):
+        self.sizes = [int(n) for n in sizes]
+        n = len(self.sizes)
+        if isinstance(params, Params):
+            params = [params] * n
+        self.params = list(params)
+        arr = (Params * n)(*self.params)
+        ns = (C.c_int * n)(*self.sizes)
+        h = C.c_void_p()
+        check(lib().tara_ens_open(C.byref(h), model, n, ns, arr, precision), "tara_ens_open")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().tara_ens_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __len__(self):
+        return len(self.sizes)
+
+    def _out(self, m):
+        if not 0 <= m < len(self.sizes):
+            raise TaraError(f"no ensemble member {m}")
+        N = self.sizes[m]
+        return [np.zeros((N, N // 2 + 1), dtype=np.complex128) for _ in range(3)]
+
+    def set_state(self, m: int, fields) -> None:
+        N = self.sizes[m]
+        a = [np.ascontiguousarray(f, dtype=np.complex128) for f in fields]
+        assert len(a) == 3 and all(x.shape == (N, N // 2 + 1) for x in a)
+        check(lib().tara_ens_set_state(self._h, m, _ptrs(a)), "tara_ens_set_state")
+
+    def get_state(self, m: int):
+        out = self._out(m)
+        check(lib().tara_ens_get_state(self._h, m, _ptrs(out)), "tara_ens_get_state")
+        return out
+
+    def get_history(self, m: int):
+        out = self._out(m)
+        check(lib().tara_ens_get_history(self._h, m, _ptrs(out)), "tara_ens_get_history")
+        return out
+
+    def step(self, stepper: int, nsteps: int) -> None:
+        check(lib().tara_ens_step(self._h, stepper, nsteps), "tara_ens_step")
+
+    def time_steps(self, stepper: int, nsteps: int) -> float:
+        ms = C.c_float()
+        check(lib().tara_ens_time_steps(self._h, stepper, nsteps, C.byref(ms)), "tara_ens_time_steps")
+        return ms.value
+
+    def set_tuning(self, tuning) -> None:
+        t = (C.c_int * 6)(*tuning)
+        check(lib().tara_ens_set_tuning(self._h, t), "tara_ens_set_tuning")
+
+    def get_tuning(self):
+        t = (C.c_int * 6)()
+        check(lib().tara_ens_get_tuning(self._h, t), "tara_ens_get_tuning")
+        return list(t)
+
+    def autotune(self, stepper: int = STEP_AB2, reps: int = 3):
+        """Pick the fastest tuning per phase; returns (tuning, ms per step of each phase)."""
+        t = (C.c_int * 6)()
+        ms = (C.c_float * 3)()
+        check(lib().tara_ens_autotune(self._h, stepper, reps, t, ms), "tara_ens_autotune")
+        return list(t), list(ms)
+
+    def diagnostics(self, m: int):
+        ns = lib().tara_ens_num_shells(self._h, m)
+        out = np.zeros(DIAG_VALUES)
+        ek = np.zeros(ns)
+        check(lib().tara_ens_diagnostics(self._h, m, out.ctypes.data, DIAG_VALUES, ek.ctypes.data, ns),
+              "tara_ens_diagnostics")
+        return out, ek
 
 
 def legacy_call(name: str, Nx: int, Ny: int, pi: float, time: float, arrays) -> int:

@@ -29,19 +29,20 @@ template <class T> struct RowCohArgs {
 // One group per transform.  Phase 1: eleven c2r in eleven groups (each
 // group's output array is its exchange buffer).  Phase 2: the products, in
 // place.  Phase 3: three r2c, exchange buffers in the freed arrays 3..5.
+// Rows y0 + (thread row) of the CTA; every thread of the CTA takes part
+// (blockDim = rows * 11 * M/P), smem holds rows * 11 arrays.
 template <class T, int M, int P>
-__global__ void __launch_bounds__(TARA_ROW_LB(11 * (M / P))) k_row_coh(const RowCohArgs<T> a) {
+__device__ __forceinline__ void row_coh_rows(const RowCohArgs<T>& a, int y0, Cx<T>* smem) {
   using RF = RowFFT<M, P>;
   constexpr int NTR = M / P, G = 11, ARR = RF::SMEM_ELEMS;
-  extern __shared__ __align__(16) unsigned char smraw[];
   const RowThread<NTR, G> th;
   const auto sync = th.sync();
   const Tables<T>& tb = a.tb;
-  Cx<T>* base = reinterpret_cast<Cx<T>*>(smraw) + (size_t)th.row * G * ARR;
+  Cx<T>* base = smem + (size_t)th.row * G * ARR;
   // 0 n, 1 ux, 2 uy, 3 dn/dx, 4 dn/dy, 5 dux/dx, 6 dux/dy, 7 duy/dx, 8 duy/dy,
   // 9 mux d2ux/dx2 + muy d2ux/dy2, 10 mux d2uy/dx2 + muy d2uy/dy2   (pairs x[2m], x[2m+1])
   auto arr = [&](int q) { return base + q * ARR; };
-  const int y = blockIdx.x * a.rb + th.row;
+  const int y = y0 + th.row;
   const size_t ro = (size_t)y * tb.ld;
   const Cx<T>* Hn = a.H[0] + ro;
   const Cx<T>* Hny = a.H[1] + ro;
@@ -110,6 +111,12 @@ __global__ void __launch_bounds__(TARA_ROW_LB(11 * (M / P))) k_row_coh(const Row
     Cx<T>* xo = a.X[g] + ro;
     row_r2c_finish<RF>(arr(3 + g), th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
   }
+}
+
+template <class T, int M, int P>
+__global__ void __launch_bounds__(TARA_ROW_LB(11 * (M / P))) k_row_coh(const RowCohArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  row_coh_rows<T, M, P>(a, blockIdx.x * a.rb, reinterpret_cast<Cx<T>*>(smraw));
 }
 
 template <int Nx, class T>

@@ -1,0 +1,698 @@
+// Batched ensembles: many independent hydro (*2coh) runs of different grid
+// sizes and viscosities advanced together.
+//
+// Layout: one arena holds every member's fields back to back, each member a
+// block of 20 fields [u_A(3) u_B(3) dold(3) | H(8) X(3)] in its own [N][ld]
+// layout; a device table of member descriptors (the argument blocks of the
+// three RHS phases, with the state buffers of both parities) drives three
+// persistent kernels per step:
+//
+//   k_ens_col_inv  items (member, column tile, job): y-inverse, 8 jobs/member
+//   k_ens_row      items (member, block of rows): the hydro row pass
+//   k_ens_col_fwd  items (member, column tile, field): y-forward, mask, AB2
+//
+// Each kernel runs a grid of (CTAs per SM) x (SMs) CTAs that walk a
+// size-sorted item list (largest grids first), so members of every size share
+// every launch; the phase boundaries are the only synchronisation.  A step is
+// the same three launches for any mix of members, so step pairs are captured
+// once into a CUDA graph and replayed.  Per-member arithmetic is the same
+// device code as a single-grid session (col_inv_tile, row_coh_rows,
+// col_fwd_simple_tile), so with the session's values-per-thread choice a
+// member's state is bit-identical to a session run of that member.
+//
+// Tuning (the autotuner picks by timing): values per thread of the column
+// passes and of the row pass (8 or 16; 384-point transforms always use 24)
+// and CTAs per SM of each persistent grid.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <vector>
+#include "coh_impl.cuh"
+#include "diag.cuh"
+
+using namespace tara;
+
+namespace {
+
+constexpr int kEnsColThreads = 256;
+constexpr int kEnsRowThreads = 352;  // 11 groups x 32
+constexpr int kEnsFields = 20;
+enum { EF_UA = 0, EF_UB = 3, EF_DOLD = 6, EF_H = 9, EF_X = 17 };
+
+// kx columns per column item: CB * L / P = 256 threads
+template <int L, int PC> struct EnsCol {
+  static constexpr int P = L == 384 ? 24 : PC;
+  static constexpr int CB = kEnsColThreads * P / L;
+};
+// rows per row item: rows * 11 * (M / P) = 352 threads
+template <int N, int PR> struct EnsRow {
+  static constexpr int M = N / 2;
+  static constexpr int P = N == 384 ? 24 : PR;
+  static constexpr int ROWS = kEnsRowThreads / (11 * (M / P));
+};
+
+template <class T> struct EnsMember {
+  ColInvArgs<T> inv[2];         // parity p: jobs read the state in buffer p
+  RowCohArgs<T> row;
+  ColFwdSimpleArgs<T> fwd[2];   // parity p: state p -> state 1-p, AB2/Euler history
+  int N;
+};
+
+#define TARA_ENS_SIZES(FN, ...) \
+  case 128: FN(128, __VA_ARGS__); break; \
+  case 256: FN(256, __VA_ARGS__); break; \
+  case 384: FN(384, __VA_ARGS__); break; \
+  case 512: FN(512, __VA_ARGS__); break;
+
+// The item's argument block is copied into shared memory, where every
+// thread reads it at broadcast speed (the structs hold only pointers, sizes
+// and scalars, so a word copy is a valid copy).
+template <class A>
+__device__ __forceinline__ void stage_args(A* dst, const A* src) {
+  static_assert(sizeof(A) % 4 == 0, "argument block is not a whole number of words");
+  const unsigned* s = reinterpret_cast<const unsigned*>(src);
+  unsigned* d = reinterpret_cast<unsigned*>(dst);
+  for (int k = threadIdx.x; k < (int)(sizeof(A) / 4); k += blockDim.x) d[k] = __ldg(s + k);
+  __syncthreads();
+}
+
+template <class T, int PC>
+__global__ void __launch_bounds__(kEnsColThreads, 2) k_ens_col_inv(const EnsMember<T>* __restrict__ mem,
+                                                                 const int4* __restrict__ items, int nitems,
+                                                                 int parity) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+  __shared__ __align__(16) ColInvArgs<T> a;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    stage_args(&a, &mem[w.x].inv[parity]);
+#define TARA_ENS_INV(L, _)                                                                          \
+  col_inv_tile<T, L, EnsCol<L, PC>::CB, EnsCol<L, PC>::P>(a.job[w.z], a.tb, w.y * EnsCol<L, PC>::CB, sm, \
+                                                          threadIdx.x)
+    switch (mem[w.x].N) { TARA_ENS_SIZES(TARA_ENS_INV, 0) }
+#undef TARA_ENS_INV
+    __syncthreads();
+  }
+}
+
+template <class T, int PR>
+__global__ void __launch_bounds__(kEnsRowThreads) k_ens_row(const EnsMember<T>* __restrict__ mem,
+                                                             const int4* __restrict__ items, int nitems) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+  __shared__ __align__(16) RowCohArgs<T> a;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    stage_args(&a, &mem[w.x].row);
+#define TARA_ENS_ROW(N, _) \
+  row_coh_rows<T, EnsRow<N, PR>::M, EnsRow<N, PR>::P>(a, w.y * EnsRow<N, PR>::ROWS, sm)
+    switch (mem[w.x].N) { TARA_ENS_SIZES(TARA_ENS_ROW, 0) }
+#undef TARA_ENS_ROW
+    __syncthreads();
+  }
+}
+
+template <class T, int PC>
+__global__ void __launch_bounds__(kEnsColThreads, 2) k_ens_col_fwd(const EnsMember<T>* __restrict__ mem,
+                                                                 const int4* __restrict__ items, int nitems,
+                                                                 int parity) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+  __shared__ __align__(16) ColFwdSimpleArgs<T> a;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    stage_args(&a, &mem[w.x].fwd[parity]);
+#define TARA_ENS_FWD(L, _) \
+  col_fwd_simple_tile<T, L, EnsCol<L, PC>::CB, EnsCol<L, PC>::P>(a, w.z, w.y * EnsCol<L, PC>::CB, sm, threadIdx.x)
+    switch (mem[w.x].N) { TARA_ENS_SIZES(TARA_ENS_FWD, 0) }
+#undef TARA_ENS_FWD
+    __syncthreads();
+  }
+}
+
+template <class T, int PC> size_t ens_col_smem() {
+  size_t m = 0;
+  m = std::max(m, (size_t)FFTB<128, EnsCol<128, PC>::CB, EnsCol<128, PC>::P>::SMEM_ELEMS);
+  m = std::max(m, (size_t)FFTB<256, EnsCol<256, PC>::CB, EnsCol<256, PC>::P>::SMEM_ELEMS);
+  m = std::max(m, (size_t)FFTB<384, EnsCol<384, PC>::CB, EnsCol<384, PC>::P>::SMEM_ELEMS);
+  m = std::max(m, (size_t)FFTB<512, EnsCol<512, PC>::CB, EnsCol<512, PC>::P>::SMEM_ELEMS);
+  return m * sizeof(Cx<T>);
+}
+template <class T, int PR> size_t ens_row_smem() {
+  size_t m = 0;
+#define TARA_ENS_RS(N) \
+  m = std::max(m, (size_t)EnsRow<N, PR>::ROWS * 11 * RowFFT<EnsRow<N, PR>::M, EnsRow<N, PR>::P>::SMEM_ELEMS)
+  TARA_ENS_RS(128);
+  TARA_ENS_RS(256);
+  TARA_ENS_RS(384);
+  TARA_ENS_RS(512);
+#undef TARA_ENS_RS
+  return m * sizeof(Cx<T>);
+}
+int ens_cb(int N, int pc) { return N == 384 ? kEnsColThreads * 24 / 384 : kEnsColThreads * pc / N; }
+int ens_rows(int N, int pr) { return kEnsRowThreads / (11 * ((N / 2) / (N == 384 ? 24 : pr))); }
+
+__global__ void k_ens_f64_to_f32(const double2* __restrict__ src, Cx<float>* dst, int Nh, int ld, int Ny) {
+  const size_t n = (size_t)Nh * Ny;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+    dst[(q / Nh) * ld + q % Nh] = cx<float>((float)src[q].x, (float)src[q].y);
+}
+__global__ void k_ens_f32_to_f64(const Cx<float>* src, double2* __restrict__ dst, int Nh, int ld, int Ny) {
+  const size_t n = (size_t)Nh * Ny;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    const Cx<float> v = src[(q / Nh) * ld + q % Nh];
+    dst[q] = make_double2((double)v.x, (double)v.y);
+  }
+}
+
+}  // namespace
+
+struct tara_ensemble {
+  int precision = TARA_FP32;
+  int n = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[8] = {};
+  int status = TARA_OK;
+  virtual ~tara_ensemble() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+  virtual int init(const int* N, const tara_params* p) = 0;
+  virtual int set_state(int m, const double* const* f, int which) = 0;
+  virtual int get_state(int m, double* const* f, int which) = 0;
+  virtual int step(int stepper, int nsteps) = 0;
+  virtual int set_tuning(const int* t) = 0;
+  virtual void get_tuning(int* t) const = 0;
+  virtual int time_phases(int stepper, int reps, float* ms3) = 0;
+  virtual int save_state(bool restore) = 0;
+  virtual int diagnostics(int m, double* out, int nout, double* Ek, int nbins) = 0;
+  virtual int num_shells(int m) = 0;
+  virtual int device_status() = 0;
+};
+
+namespace {
+
+template <class T>
+struct EnsembleT : tara_ensemble {
+  std::vector<int> N;
+  std::vector<tara_params> prm;
+  std::map<int, std::unique_ptr<Grid<T>>> grids;        // tables per grid size
+  std::map<int, std::unique_ptr<DiagWork<T>>> diags;
+  std::vector<size_t> off;                                // element offset of each member block
+  std::vector<size_t> elems;                              // elements per field of each member
+  Cx<T>* arena = nullptr;
+  double* stage = nullptr;                                // FP64 host-layout staging (largest member)
+  double* drec = nullptr;                                 // one diagnostics record
+  EnsMember<T>* dmem = nullptr;
+  std::vector<EnsMember<T>> hmem;
+  int4* ditems[3] = {nullptr, nullptr, nullptr};
+  int nitems[3] = {0, 0, 0};
+  int tuning[6] = {16, 16, 16, 0, 0, 0};  // P col_inv, P row, P col_fwd, CTAs/SM of each (0 = most that fit)
+  int parity = 0;
+  int built_mode = -1;
+  Cx<T>* backup = nullptr;
+  size_t backup_elems = 0;
+  int saved_parity = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_mode = -1, graph_parity = -1;
+
+  ~EnsembleT() override {
+    if (st) cudaStreamSynchronize(st);
+    drop_graph();
+    for (auto& d : diags) d.second->release();
+    for (auto& g : grids) g.second->release();
+    for (auto& p : ditems)
+      if (p) cudaFree(p);
+    if (dmem) cudaFree(dmem);
+    if (arena) cudaFree(arena);
+    if (stage) cudaFree(stage);
+    if (drec) cudaFree(drec);
+    if (backup) cudaFree(backup);
+  }
+  void drop_graph() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    graph_mode = graph_parity = -1;
+  }
+  Cx<T>* field(int m, int f) const { return arena + off[m] + (size_t)f * elems[m]; }
+
+  int init(const int* Nin, const tara_params* p) override {
+    N.assign(Nin, Nin + n);
+    prm.assign(p, p + n);
+    size_t total = 0, maxh = 0;
+    off.resize(n);
+    elems.resize(n);
+    for (int m = 0; m < n; m++) {
+      if (N[m] != 128 && N[m] != 256 && N[m] != 384 && N[m] != 512) {
+        set_error("ensemble member grid sizes must be 128, 256, 384 or 512");
+        return TARA_EUNSUPPORTED;
+      }
+      auto& g = grids[N[m]];
+      if (!g) {
+        g.reset(new Grid<T>());
+        TARA_TRY(g->init(N[m], N[m], p[m].Lx, p[m].Ly, p[m].pi, st));
+      } else if (g->Lx != p[m].Lx || g->Ly != p[m].Ly || g->pi != p[m].pi) {
+        set_error("ensemble members of one grid size must share Lx, Ly and pi");
+        return TARA_EINVAL;
+      }
+      off[m] = total;
+      elems[m] = g->field_elems();
+      total += elems[m] * kEnsFields;
+      maxh = std::max(maxh, (size_t)(N[m] / 2 + 1) * N[m]);
+    }
+    if (cudaMalloc(&arena, total * sizeof(Cx<T>)) != cudaSuccess) {
+      arena = nullptr;
+      set_error("cudaMalloc of the ensemble arena (" + std::to_string(total * sizeof(Cx<T>)) + " bytes) failed");
+      return TARA_ENOMEM;
+    }
+    TARA_CUDA_TRY(cudaMemsetAsync(arena, 0, total * sizeof(Cx<T>), st));
+    TARA_CUDA_TRY(cudaMalloc(&stage, maxh * sizeof(Cx<double>)));
+    TARA_CUDA_TRY(cudaMalloc(&drec, (kDiagOut + 1024) * sizeof(double)));
+    TARA_CUDA_TRY(cudaMalloc(&dmem, (size_t)n * sizeof(EnsMember<T>)));
+    build_members();
+    TARA_CUDA_TRY(cudaMemcpyAsync(dmem, hmem.data(), (size_t)n * sizeof(EnsMember<T>), cudaMemcpyHostToDevice, st));
+    TARA_TRY(build_items());
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+
+  void build_members() {
+    hmem.assign(n, EnsMember<T>{});
+    for (int m = 0; m < n; m++) {
+      EnsMember<T>& e = hmem[m];
+      const Tables<T>& tb = grids[N[m]]->tb;
+      e.N = N[m];
+      const int src[8] = {0, 0, 1, 1, 1, 2, 2, 2};
+      const int mul[8] = {MUL_ONE, MUL_IKY, MUL_ONE, MUL_IKY, MUL_KY2, MUL_ONE, MUL_IKY, MUL_KY2};
+      for (int par = 0; par < 2; par++) {
+        const int ubase = par ? EF_UB : EF_UA, nbase = par ? EF_UA : EF_UB;
+        e.inv[par].tb = tb;
+        for (int q = 0; q < 8; q++) e.inv[par].job[q] = ColInvJob<T>{field(m, ubase + src[q]), field(m, EF_H + q), mul[q], (T)0};
+        ColFwdSimpleArgs<T>& f = e.fwd[par];
+        f.tb = tb;
+        for (int q = 0; q < 3; q++) {
+          f.X[q] = field(m, EF_X + q);
+          f.sign[q] = (T)-1;
+          f.step.u[q] = field(m, ubase + q);
+          f.step.unew[q] = field(m, nbase + q);
+          f.step.dold[q] = field(m, EF_DOLD + q);
+        }
+        f.step.dt = (T)prm[m].dt;
+      }
+      e.row.tb = tb;
+      for (int q = 0; q < 8; q++) e.row.H[q] = field(m, EF_H + q);
+      for (int q = 0; q < 3; q++) e.row.X[q] = field(m, EF_X + q);
+      e.row.mux = (T)prm[m].mux;
+      e.row.muy = (T)prm[m].muy;
+      e.row.cs2 = (T)(prm[m].CS * prm[m].CS);
+    }
+  }
+  int set_mode(int mode) {
+    if (mode == built_mode) return TARA_OK;
+    for (auto& e : hmem)
+      for (auto& f : e.fwd) f.step.mode = mode;
+    TARA_CUDA_TRY(cudaMemcpyAsync(dmem, hmem.data(), (size_t)n * sizeof(EnsMember<T>), cudaMemcpyHostToDevice, st));
+    built_mode = mode;
+    return TARA_OK;
+  }
+
+  int build_items() {
+    std::vector<int> order(n);
+    for (int m = 0; m < n; m++) order[m] = m;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return N[a] > N[b]; });
+    std::vector<int4> it[3];
+    for (int m : order) {
+      const int Nh = N[m] / 2 + 1;
+      const int ti = (Nh + ens_cb(N[m], tuning[0]) - 1) / ens_cb(N[m], tuning[0]);
+      for (int t = 0; t < ti; t++)
+        for (int j = 0; j < 8; j++) it[0].push_back(make_int4(m, t, j, 0));
+      const int rows = ens_rows(N[m], tuning[1]);
+      for (int r = 0; r < N[m] / rows; r++) it[1].push_back(make_int4(m, r, 0, 0));
+      const int tf = (Nh + ens_cb(N[m], tuning[2]) - 1) / ens_cb(N[m], tuning[2]);
+      for (int t = 0; t < tf; t++)
+        for (int f = 0; f < 3; f++) it[2].push_back(make_int4(m, t, f, 0));
+    }
+    for (int k = 0; k < 3; k++) {
+      if (ditems[k]) cudaFree(ditems[k]);
+      ditems[k] = nullptr;
+      nitems[k] = (int)it[k].size();
+      TARA_CUDA_TRY(cudaMalloc(&ditems[k], it[k].size() * sizeof(int4)));
+      TARA_CUDA_TRY(cudaMemcpyAsync(ditems[k], it[k].data(), it[k].size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    }
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+
+  template <class K>
+  int grid_of(K kern, int threads, size_t smem, int want, int& grid) {
+    if (smem > 48 * 1024) TARA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per = 0;
+    TARA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem));
+    if (per < 1) { set_error("ensemble kernel does not fit on a multiprocessor"); return TARA_EUNSUPPORTED; }
+    if (want > 0 && want < per) per = want;
+    grid = per * grids.begin()->second->tb.sm_count;
+    return TARA_OK;
+  }
+  int launch_inv(int par) {
+    int grid = 0;
+    if (tuning[0] == 8) {
+      const size_t smem = ens_col_smem<T, 8>();
+      TARA_TRY(grid_of(k_ens_col_inv<T, 8>, kEnsColThreads, smem, tuning[3], grid));
+      k_ens_col_inv<T, 8><<<std::min(grid, nitems[0]), kEnsColThreads, smem, st>>>(dmem, ditems[0], nitems[0], par);
+    } else {
+      const size_t smem = ens_col_smem<T, 16>();
+      TARA_TRY(grid_of(k_ens_col_inv<T, 16>, kEnsColThreads, smem, tuning[3], grid));
+      k_ens_col_inv<T, 16><<<std::min(grid, nitems[0]), kEnsColThreads, smem, st>>>(dmem, ditems[0], nitems[0], par);
+    }
+    return TARA_OK;
+  }
+  int launch_row() {
+    int grid = 0;
+    if (tuning[1] == 8) {
+      const size_t smem = ens_row_smem<T, 8>();
+      TARA_TRY(grid_of(k_ens_row<T, 8>, kEnsRowThreads, smem, tuning[4], grid));
+      k_ens_row<T, 8><<<std::min(grid, nitems[1]), kEnsRowThreads, smem, st>>>(dmem, ditems[1], nitems[1]);
+    } else {
+      const size_t smem = ens_row_smem<T, 16>();
+      TARA_TRY(grid_of(k_ens_row<T, 16>, kEnsRowThreads, smem, tuning[4], grid));
+      k_ens_row<T, 16><<<std::min(grid, nitems[1]), kEnsRowThreads, smem, st>>>(dmem, ditems[1], nitems[1]);
+    }
+    return TARA_OK;
+  }
+  int launch_fwd(int par) {
+    int grid = 0;
+    if (tuning[2] == 8) {
+      const size_t smem = ens_col_smem<T, 8>();
+      TARA_TRY(grid_of(k_ens_col_fwd<T, 8>, kEnsColThreads, smem, tuning[5], grid));
+      k_ens_col_fwd<T, 8><<<std::min(grid, nitems[2]), kEnsColThreads, smem, st>>>(dmem, ditems[2], nitems[2], par);
+    } else {
+      const size_t smem = ens_col_smem<T, 16>();
+      TARA_TRY(grid_of(k_ens_col_fwd<T, 16>, kEnsColThreads, smem, tuning[5], grid));
+      k_ens_col_fwd<T, 16><<<std::min(grid, nitems[2]), kEnsColThreads, smem, st>>>(dmem, ditems[2], nitems[2], par);
+    }
+    return TARA_OK;
+  }
+  int launch_steps(int n_) {
+    for (int s = 0; s < n_; s++) {
+      TARA_TRY(launch_inv(parity));
+      TARA_TRY(launch_row());
+      TARA_TRY(launch_fwd(parity));
+      TARA_CUDA_TRY(cudaGetLastError());
+      parity ^= 1;
+    }
+    return TARA_OK;
+  }
+  int step(int stepper, int nsteps) override {
+    if (stepper != TARA_STEP_AB2 && stepper != TARA_STEP_EULER) {
+      set_error("ensembles step with AB2 or Euler");
+      return TARA_EINVAL;
+    }
+    const int mode = stepper == TARA_STEP_AB2 ? STEP_AB2 : STEP_EULER;
+    if (mode != built_mode) {
+      drop_graph();
+      TARA_TRY(set_mode(mode));
+    }
+    int done = 0;
+    if (nsteps >= 2) {
+      if (!graph || graph_mode != mode || graph_parity != parity) {
+        drop_graph();
+        const int p0 = parity;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+          const int r = launch_steps(2);
+          const cudaError_t e = cudaStreamEndCapture(st, &g);
+          if (r == TARA_OK && e == cudaSuccess && g && cudaGraphInstantiate(&graph, g, 0) != cudaSuccess) graph = nullptr;
+          if (g) cudaGraphDestroy(g);
+          cudaGetLastError();
+        }
+        parity = p0;  // nothing ran while capturing
+        if (graph) {
+          graph_mode = mode;
+          graph_parity = parity;
+        }
+      }
+      if (graph)
+        for (; done + 2 <= nsteps; done += 2) TARA_CUDA_TRY(cudaGraphLaunch(graph, st));
+    }
+    return launch_steps(nsteps - done);
+  }
+
+  int set_tuning(const int* t) override {
+    for (int k = 0; k < 3; k++)
+      if (t[k] != 8 && t[k] != 16) { set_error("values per thread must be 8 or 16"); return TARA_EINVAL; }
+    for (int k = 3; k < 6; k++)
+      if (t[k] < 0) { set_error("CTAs per SM must be >= 0"); return TARA_EINVAL; }
+    const bool items_change = t[0] != tuning[0] || t[1] != tuning[1] || t[2] != tuning[2];
+    std::memcpy(tuning, t, sizeof(tuning));
+    drop_graph();
+    if (items_change) TARA_TRY(build_items());
+    return TARA_OK;
+  }
+  void get_tuning(int* t) const override { std::memcpy(t, tuning, sizeof(tuning)); }
+
+  // device time of each phase summed over `reps` steps (host launches)
+  int time_phases(int stepper, int reps, float* ms3) override {
+    const int mode = stepper == TARA_STEP_AB2 ? STEP_AB2 : STEP_EULER;
+    drop_graph();
+    TARA_TRY(set_mode(mode));
+    for (int k = 0; k < 3; k++) ms3[k] = 0;
+    for (auto& e : ev)
+      if (!e) TARA_CUDA_TRY(cudaEventCreate(&e));
+    for (int r = 0; r < reps; r++) {
+      TARA_CUDA_TRY(cudaEventRecord(ev[0], st));
+      TARA_TRY(launch_inv(parity));
+      TARA_CUDA_TRY(cudaEventRecord(ev[1], st));
+      TARA_TRY(launch_row());
+      TARA_CUDA_TRY(cudaEventRecord(ev[2], st));
+      TARA_TRY(launch_fwd(parity));
+      TARA_CUDA_TRY(cudaEventRecord(ev[3], st));
+      TARA_CUDA_TRY(cudaEventSynchronize(ev[3]));
+      for (int k = 0; k < 3; k++) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+        ms3[k] += t;
+      }
+      parity ^= 1;
+    }
+    return device_status();
+  }
+  // copy of every member's state and AB2 history (restore = true puts it back)
+  int save_state(bool restore) override {
+    size_t need = 0;
+    for (int m = 0; m < n; m++) need += 9 * elems[m];
+    if (!restore) {
+      if (!backup) {
+        if (cudaMalloc(&backup, need * sizeof(Cx<T>)) != cudaSuccess) {
+          backup = nullptr;
+          set_error("cudaMalloc of the tuning backup failed");
+          return TARA_ENOMEM;
+        }
+        backup_elems = need;
+      }
+      saved_parity = parity;
+    } else if (!backup) {
+      set_error("no saved state");
+      return TARA_EINVAL;
+    }
+    size_t o = 0;
+    for (int m = 0; m < n; m++) {
+      const size_t b = 9 * elems[m] * sizeof(Cx<T>);
+      if (restore) TARA_CUDA_TRY(cudaMemcpyAsync(field(m, 0), backup + o, b, cudaMemcpyDeviceToDevice, st));
+      else TARA_CUDA_TRY(cudaMemcpyAsync(backup + o, field(m, 0), b, cudaMemcpyDeviceToDevice, st));
+      o += 9 * elems[m];
+    }
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (restore) {
+      cudaFree(backup);
+      backup = nullptr;
+      parity = saved_parity;
+      drop_graph();
+    }
+    return TARA_OK;
+  }
+
+  int device_status() override {
+    int v = 0;
+    for (auto& g : grids) {
+      int s = 0;
+      TARA_CUDA_TRY(cudaMemcpyAsync(&s, g.second->tb.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+      TARA_CUDA_TRY(cudaStreamSynchronize(st));
+      if (s != TARA_OK) {
+        const int zero = 0;
+        cudaMemcpyAsync(g.second->tb.status, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+        v = s;
+      }
+    }
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (v) set_error("a bounded wait ran out in a kernel");
+    return v;
+  }
+
+  // which: 0 state, 1 AB2 history
+  Cx<T>* fptr(int m, int which, int q) { return field(m, which ? EF_DOLD + q : (parity ? EF_UB : EF_UA) + q); }
+  int set_state(int m, const double* const* h, int which) override {
+    if (m < 0 || m >= n || !h) { set_error("bad member or null field array"); return TARA_EINVAL; }
+    const int Nh = N[m] / 2 + 1, ld = grids[N[m]]->ld;
+    for (int q = 0; q < 3; q++) {
+      if (!h[q]) { set_error("null host field pointer"); return TARA_EINVAL; }
+      if constexpr (sizeof(T) == sizeof(double)) {
+        TARA_CUDA_TRY(cudaMemcpy2DAsync(fptr(m, which, q), ld * sizeof(Cx<T>), h[q], Nh * sizeof(Cx<double>),
+                                        Nh * sizeof(Cx<double>), N[m], cudaMemcpyHostToDevice, st));
+      } else {
+        TARA_CUDA_TRY(cudaMemcpyAsync(stage, h[q], (size_t)Nh * N[m] * sizeof(Cx<double>), cudaMemcpyHostToDevice, st));
+        k_ens_f64_to_f32<<<256, 256, 0, st>>>(reinterpret_cast<const double2*>(stage),
+                                              reinterpret_cast<Cx<float>*>(fptr(m, which, q)), Nh, ld, N[m]);
+        TARA_CUDA_TRY(cudaGetLastError());
+      }
+    }
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+  int get_state(int m, double* const* h, int which) override {
+    if (m < 0 || m >= n || !h) { set_error("bad member or null field array"); return TARA_EINVAL; }
+    const int Nh = N[m] / 2 + 1, ld = grids[N[m]]->ld;
+    for (int q = 0; q < 3; q++) {
+      if (!h[q]) { set_error("null host field pointer"); return TARA_EINVAL; }
+      if constexpr (sizeof(T) == sizeof(double)) {
+        TARA_CUDA_TRY(cudaMemcpy2DAsync(h[q], Nh * sizeof(Cx<double>), fptr(m, which, q), ld * sizeof(Cx<T>),
+                                        Nh * sizeof(Cx<double>), N[m], cudaMemcpyDeviceToHost, st));
+      } else {
+        k_ens_f32_to_f64<<<256, 256, 0, st>>>(reinterpret_cast<const Cx<float>*>(fptr(m, which, q)),
+                                              reinterpret_cast<double2*>(stage), Nh, ld, N[m]);
+        TARA_CUDA_TRY(cudaGetLastError());
+        TARA_CUDA_TRY(cudaMemcpyAsync(h[q], stage, (size_t)Nh * N[m] * sizeof(Cx<double>), cudaMemcpyDeviceToHost, st));
+      }
+      TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return device_status();
+  }
+
+  int num_shells(int m) override {
+    if (m < 0 || m >= n) return 0;
+    return diag_num_shells(N[m], N[m], prm[m].Lx, prm[m].Ly, prm[m].pi);
+  }
+  int diagnostics(int m, double* out, int nout, double* Ek, int nbins) override {
+    if (m < 0 || m >= n) { set_error("bad member"); return TARA_EINVAL; }
+    const int ns = num_shells(m);
+    if (nout > kDiagOut || nbins > ns || ns > 1024) { set_error("more values requested than computed"); return TARA_EINVAL; }
+    Grid<T>& g = *grids[N[m]];
+    auto& dw = diags[N[m]];
+    if (!dw) {
+      dw.reset(new DiagWork<T>());
+      TARA_TRY(dw->alloc(g, st));
+    }
+    FieldPool<T> H{field(m, EF_H), elems[m], 8}, X{field(m, EF_X), elems[m], 3};
+    Cx<T>* state[3] = {fptr(m, 0, 0), fptr(m, 0, 1), fptr(m, 0, 2)};
+    TARA_TRY(diag_record(TARA_MODEL_COH, g, *dw, state, H, X, X, drec, st));
+    std::vector<double> rec(kDiagOut + ns);
+    TARA_CUDA_TRY(cudaMemcpyAsync(rec.data(), drec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int k = 0; k < nout; k++) out[k] = rec[k];
+    for (int k = 0; k < nbins; k++) Ek[k] = rec[kDiagOut + k];
+    return device_status();
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int tara_ens_open(tara_ensemble** out, int model, int n, const int* N, const tara_params* params, int precision) {
+  if (!out || !N || !params || n < 1) { set_error("null argument or empty ensemble"); return TARA_EINVAL; }
+  *out = nullptr;
+  if (model != TARA_MODEL_COH) { set_error("ensembles run the hydro model"); return TARA_EUNSUPPORTED; }
+  if (precision != TARA_FP32 && precision != TARA_FP64) { set_error("unknown precision"); return TARA_EINVAL; }
+  std::unique_ptr<tara_ensemble> e(precision == TARA_FP32 ? (tara_ensemble*)new EnsembleT<float>()
+                                                          : (tara_ensemble*)new EnsembleT<double>());
+  e->precision = precision;
+  e->n = n;
+  if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cudaStreamCreate failed");
+    return TARA_ECUDA;
+  }
+  const int r = e->init(N, params);
+  if (r != TARA_OK) return r;
+  *out = e.release();
+  return TARA_OK;
+}
+int tara_ens_close(tara_ensemble* e) {
+  if (!e) return TARA_EINVAL;
+  delete e;
+  return TARA_OK;
+}
+int tara_ens_size(const tara_ensemble* e) { return e ? e->n : 0; }
+int tara_ens_set_state(tara_ensemble* e, int m, const double* const* f) { return e ? e->set_state(m, f, 0) : TARA_EINVAL; }
+int tara_ens_get_state(tara_ensemble* e, int m, double* const* f) { return e ? e->get_state(m, f, 0) : TARA_EINVAL; }
+int tara_ens_get_history(tara_ensemble* e, int m, double* const* f) { return e ? e->get_state(m, f, 1) : TARA_EINVAL; }
+int tara_ens_step(tara_ensemble* e, int stepper, int nsteps) {
+  if (!e || nsteps < 0) return TARA_EINVAL;
+  return e->step(stepper, nsteps);
+}
+int tara_ens_time_steps(tara_ensemble* e, int stepper, int nsteps, float* ms) {
+  if (!e || !ms || nsteps < 0) return TARA_EINVAL;
+  if (cudaStreamSynchronize(e->st) != cudaSuccess) return TARA_ECUDA;
+  for (int k = 0; k < 2; k++)
+    if (!e->ev[4 + k] && cudaEventCreate(&e->ev[4 + k]) != cudaSuccess) return TARA_ECUDA;
+  cudaEventRecord(e->ev[4], e->st);
+  int r = e->step(stepper, nsteps);
+  if (r != TARA_OK) return r;
+  cudaEventRecord(e->ev[5], e->st);
+  if (cudaEventSynchronize(e->ev[5]) != cudaSuccess) {
+    set_error("cudaEventSynchronize failed");
+    return TARA_ECUDA;
+  }
+  cudaEventElapsedTime(ms, e->ev[4], e->ev[5]);
+  return e->device_status();
+}
+int tara_ens_set_tuning(tara_ensemble* e, const int* t) { return e && t ? e->set_tuning(t) : TARA_EINVAL; }
+int tara_ens_get_tuning(const tara_ensemble* e, int* t) {
+  if (!e || !t) return TARA_EINVAL;
+  e->get_tuning(t);
+  return TARA_OK;
+}
+
+// Times each phase kernel under every candidate (values per thread 8/16,
+// 1, 2 or all CTAs per SM that fit) on the ensemble's own members and keeps
+// the fastest per phase.  The state and AB2 history are restored afterwards.
+int tara_ens_autotune(tara_ensemble* e, int stepper, int reps, int* chosen, float* best_ms) {
+  if (!e || reps < 1) return TARA_EINVAL;
+  int r = e->save_state(false);
+  if (r != TARA_OK) return r;
+  int t[6];
+  e->get_tuning(t);
+  const int pvals[2] = {8, 16}, occ[3] = {1, 2, 0};
+  float best[3] = {1e30f, 1e30f, 1e30f};
+  int bestp[3] = {t[0], t[1], t[2]}, besto[3] = {t[3], t[4], t[5]};
+  for (int pi = 0; pi < 2 && r == TARA_OK; pi++)
+    for (int oi = 0; oi < 3 && r == TARA_OK; oi++) {
+      int c[6] = {pvals[pi], pvals[pi], pvals[pi], occ[oi], occ[oi], occ[oi]};
+      r = e->set_tuning(c);
+      float ms[3];
+      if (r == TARA_OK) r = e->time_phases(stepper, 1, ms);     // warm-up
+      if (r == TARA_OK) r = e->time_phases(stepper, reps, ms);
+      if (r != TARA_OK) break;
+      for (int k = 0; k < 3; k++)
+        if (ms[k] < best[k]) {
+          best[k] = ms[k];
+          bestp[k] = pvals[pi];
+          besto[k] = occ[oi];
+        }
+    }
+  const int fin[6] = {bestp[0], bestp[1], bestp[2], besto[0], besto[1], besto[2]};
+  if (r == TARA_OK) r = e->set_tuning(fin);
+  const int rr = e->save_state(true);
+  if (r == TARA_OK) r = rr;
+  if (r == TARA_OK && chosen) e->get_tuning(chosen);
+  if (r == TARA_OK && best_ms)
+    for (int k = 0; k < 3; k++) best_ms[k] = best[k] / reps;
+  return r;
+}
+int tara_ens_num_shells(tara_ensemble* e, int m) { return e ? e->num_shells(m) : 0; }
+int tara_ens_diagnostics(tara_ensemble* e, int m, double* out, int nout, double* Ek, int nbins) {
+  if (!e || (!out && nout > 0) || (!Ek && nbins > 0) || nout < 0 || nbins < 0) return TARA_EINVAL;
+  return e->diagnostics(m, out, nout, Ek, nbins);
+}
+
+}  // extern "C"

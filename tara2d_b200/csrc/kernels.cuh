@@ -109,25 +109,30 @@ template <class T> struct ColInvArgs {
   ColInvJob<T> job[8];
 };
 
-// blockIdx.x: tile of CB kx columns; blockIdx.y: job
+// y-inverse of the CB kx columns c0.. of one job, by CB*L/P threads (tid)
+// sharing the exchange tile sm.
 template <class T, int L, int CB, int P>
-__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_inv(const ColInvArgs<T> a) {
+__device__ __forceinline__ void col_inv_tile(const ColInvJob<T>& jb, const Tables<T>& tb, int c0, Cx<T>* sm,
+                                             int tid) {
   using F = FFTB<L, CB, P>;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
-  const ColInvJob<T> jb = a.job[blockIdx.y];
-  const int c0 = blockIdx.x * CB;
-  const int Nh = a.tb.Nh, ld = a.tb.ld;
+  const int Nh = tb.Nh, ld = tb.ld;
   Cx<T> v[P];
-  fft_run<F, +1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
+  fft_run<F, +1>(sm, tid, v, TwGlobal<T>{tb.tw_col}, [&](int t, int i) -> Cx<T> {
     const int c = c0 + t;
     if (c >= Nh) return cx<T>(0, 0);
-    return apply_job_mul(jb, a.tb, c, i, ldg(jb.src + (size_t)i * ld + c));
+    return apply_job_mul(jb, tb, c, i, ldg(jb.src + (size_t)i * ld + c));
   }, SyncBlock{});
-  fft_emit<F>(threadIdx.x, v, [&](int t, int i, Cx<T> x) {
+  fft_emit<F>(tid, v, [&](int t, int i, Cx<T> x) {
     const int c = c0 + t;
     if (c < Nh) st(jb.dst + (size_t)i * ld + c, x);
   });
+}
+
+// blockIdx.x: tile of CB kx columns; blockIdx.y: job
+template <class T, int L, int CB, int P>
+__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_inv(const ColInvArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  col_inv_tile<T, L, CB, P>(a.job[blockIdx.y], a.tb, blockIdx.x * CB, reinterpret_cast<Cx<T>*>(smraw), threadIdx.x);
 }
 
 // TMA-staged, persistent variant: each CTA loops over (tile, job) items; the
@@ -284,23 +289,21 @@ template <class T> struct ColFwdSimpleArgs {
   StepArgs<T> step;
 };
 
+// Output field f, kx columns c0..c0+CB-1, by CB*L/P threads (tid).
 template <class T, int L, int CB, int P>
-__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_simple(const ColFwdSimpleArgs<T> a) {
+__device__ __forceinline__ void col_fwd_simple_tile(const ColFwdSimpleArgs<T>& a, int f, int c0, Cx<T>* sm,
+                                                    int tid) {
   using F = FFTB<L, CB, P>;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
-  const int f = blockIdx.y;
-  const int c0 = blockIdx.x * CB;
   const int Nh = a.tb.Nh, ld = a.tb.ld;
   const Cx<T>* X = a.X[f];
   Cx<T> v[P];
-  fft_run<F, -1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
+  fft_run<F, -1>(sm, tid, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
     const int c = c0 + t;
     if (c >= Nh) return cx<T>(0, 0);
     return ldg(X + (size_t)i * ld + c);
   }, SyncBlock{});
   const T sg = a.sign[f];
-  fft_emit<F>(threadIdx.x, v, [&](int t, int j, Cx<T> x) {
+  fft_emit<F>(tid, v, [&](int t, int j, Cx<T> x) {
     const int c = c0 + t;
     if (c >= Nh) return;
     const bool masked = !a.nomask && c >= __ldg(a.tb.cut + j);
@@ -308,6 +311,12 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_s
     Cx<T> d = cx<T>(sg * val.x, sg * val.y);
     step_apply(a.step, f, (size_t)j * ld + c, d);
   });
+}
+
+template <class T, int L, int CB, int P>
+__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_simple(const ColFwdSimpleArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  col_fwd_simple_tile<T, L, CB, P>(a, blockIdx.y, blockIdx.x * CB, reinterpret_cast<Cx<T>*>(smraw), threadIdx.x);
 }
 
 template <class T, int L>

@@ -70,6 +70,19 @@ def coh_random_phase(Nx=128, Ny=128, seed=0, k0=4.0, energy=0.5, noise=0.01):
     return [r2c(n), r2c(ux), r2c(uy)]
 
 
+def ensemble_members(n=256, seed=0, sizes=(128, 256, 384, 512), nu_range=(1e-4, 1e-2), k0_range=(2.0, 8.0)):
+    """Seeded ensemble of hydro runs: grid size uniform over `sizes`, viscosity
+    log-uniform over `nu_range`, IC peak wavenumber k0 uniform over `k0_range`,
+    and a seed per member.  Returns a list of dicts (N, nu, k0, seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        out.append(dict(N=int(rng.choice(sizes)),
+                        nu=float(np.exp(rng.uniform(np.log(nu_range[0]), np.log(nu_range[1])))),
+                        k0=float(rng.uniform(*k0_range)), seed=int(rng.integers(0, 2 ** 31 - 1))))
+    return out
+
+
 def com_state(rho, ux, uy, Bx, By, CS, spheat=5.0 / 3.0):
     """Conservative MHD state (rho, rho ux, rho uy, E, Bx, By) in k-space with
     P = CS^2 rho and E = P/(spheat-1) + rho u^2/2 + B^2/2 (src/main2com.f95:247-255)."""
