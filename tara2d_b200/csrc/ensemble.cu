@@ -96,8 +96,11 @@ __global__ void __launch_bounds__(kEnsColThreads, 2) k_ens_col_inv(const EnsMemb
   }
 }
 
+// two row CTAs per SM in FP32 (80 registers, a few words spilled); FP64 keeps one
+template <class T> constexpr int ens_row_minb() { return sizeof(T) == 4 ? 2 : 1; }
+
 template <class T, int PR>
-__global__ void __launch_bounds__(kEnsRowThreads) k_ens_row(const EnsMember<T>* __restrict__ mem,
+__global__ void __launch_bounds__(kEnsRowThreads, ens_row_minb<T>()) k_ens_row(const EnsMember<T>* __restrict__ mem,
                                                              const int4* __restrict__ items, int nitems) {
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
