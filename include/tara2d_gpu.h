@@ -118,6 +118,24 @@ int tara_diagnostics(tara_session* s, double* out, int nout, double* Ek, int nbi
  * * every in all).  Records stay on the device until the run ends. */
 int tara_run_recorded(tara_session* s, int stepper, int every, int nrec, double* rec);
 
+/* ---- real space and the drivers' output files ----
+ * Real fields are real(8) (Nx,Ny) host arrays (x fastest).
+ * tara_get_state_real: every state field after c2r / (Nx Ny), as the drivers
+ * form them before their diagnostics (src/main2com.f95:446-480).
+ * tara_get_vorticity_real: omega = c2r(i kx uy_k - i ky ux_k)/(Nx Ny), u the
+ * velocity (src/main2coh.f95:321-360; MHD: u = (rho u)/rho, src/main2com.f95:500-540).
+ * tara_set_state_real: the state from real fields by the device r2c, the
+ * drivers' initial-condition path (src/main2com.f95:257-262).
+ * tara_write_snapshot: the drivers' grid file (`fort.NNNNNNNN`,
+ * src/main2com.f95:603-609, src/main2coh.f95:414-418), list-directed.
+ * tara_format_list_directed: one list-directed record of n REAL(8) values
+ * as gfortran writes them (for Energy.dat lines); returns its length. */
+int tara_get_state_real(tara_session* s, double* const* fields);
+int tara_get_vorticity_real(tara_session* s, double* omega);
+int tara_set_state_real(tara_session* s, const double* const* fields);
+int tara_write_snapshot(tara_session* s, const char* path);
+int tara_format_list_directed(const double* v, int n, char* out, int cap);
+
 /* ---- batched ensembles (no counterpart in the reference, whose drivers run
  * one grid per process) ----
  * n independent hydro (*2coh) runs, member m on an N[m] x N[m] grid

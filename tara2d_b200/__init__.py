@@ -91,6 +91,11 @@ def lib():
         L.tara_device_pci_bus_id.argtypes = [C.c_char_p, I]
         L.tara_set_device.argtypes = [I]
         L.tara_set_graphs.argtypes = [P, I]
+        L.tara_get_state_real.argtypes = [P, PP]
+        L.tara_set_state_real.argtypes = [P, PP]
+        L.tara_get_vorticity_real.argtypes = [P, P]
+        L.tara_write_snapshot.argtypes = [P, C.c_char_p]
+        L.tara_format_list_directed.argtypes = [P, I, C.c_char_p, I]
         L.tara_ens_open.argtypes = [C.POINTER(C.c_void_p), I, I, P, C.POINTER(Params), I]
         L.tara_ens_close.argtypes = [P]
         for n in ("tara_ens_set_state", "tara_ens_get_state", "tara_ens_get_history"):
@@ -207,6 +212,30 @@ class Session:
     def launches_per_step(self, stepper: int) -> int:
         return lib().tara_launches_per_step(self._h, stepper)
 
+    def _real_out(self, n):
+        return [np.zeros((self.Ny, self.Nx), dtype=np.float64) for _ in range(n)]
+
+    def get_state_real(self):
+        """Every state field in real space (c2r / (Nx Ny)), arrays of shape (Ny, Nx)."""
+        out = self._real_out(self.nf)
+        check(lib().tara_get_state_real(self._h, _ptrs(out)), "tara_get_state_real")
+        return out
+
+    def get_vorticity_real(self):
+        out = self._real_out(1)[0]
+        check(lib().tara_get_vorticity_real(self._h, out.ctypes.data), "tara_get_vorticity_real")
+        return out
+
+    def set_state_real(self, fields) -> None:
+        """State from real-space fields (shape (Ny, Nx)) by the device r2c."""
+        a = [np.ascontiguousarray(f, dtype=np.float64) for f in fields]
+        assert len(a) == self.nf and all(x.shape == (self.Ny, self.Nx) for x in a)
+        check(lib().tara_set_state_real(self._h, _ptrs(a)), "tara_set_state_real")
+
+    def write_snapshot(self, path: str) -> None:
+        """The drivers' grid file (fort.NNNNNNNN) of the current state."""
+        check(lib().tara_write_snapshot(self._h, os.fsencode(path)), "tara_write_snapshot")
+
     def set_graphs(self, on: bool) -> None:
         """Replay steps from CUDA graphs (default) or launch every kernel from the host."""
         check(lib().tara_set_graphs(self._h, 1 if on else 0), "tara_set_graphs")
@@ -274,6 +303,16 @@ def _i32(v):
 
 def _d(v):
     return C.byref(C.c_double(v))
+
+
+def format_list_directed(values) -> str:
+    """One Fortran list-directed record of REAL(8) values, as gfortran writes it."""
+    v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+    buf = C.create_string_buffer(32 * v.size + 8)
+    n = lib().tara_format_list_directed(v.ctypes.data, v.size, buf, len(buf))
+    if n < 0:
+        raise TaraError(f"tara_format_list_directed failed: {last_error()}")
+    return buf.value.decode()
 
 
 class Ensemble:

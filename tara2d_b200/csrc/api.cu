@@ -9,6 +9,8 @@
 #include <vector>
 #include "models.h"
 #include "diag.cuh"
+#include "output.h"
+#include "realspace.cuh"
 
 using namespace tara;
 
@@ -121,6 +123,9 @@ struct tara_session {
                                 double* out) = 0;
   virtual int num_shells() = 0;
   virtual void set_graphs(bool on) = 0;
+  // what = 0: the nf state fields in real space (c2r / NxNy); 1: vorticity
+  virtual int real_fields(int what, double* const* h) = 0;
+  virtual int set_state_real(const double* const* h) = 0;
   // nrec diagnostics records of the state, one before the first step and one
   // after every `every` steps (nsteps = (nrec - 1) * every), into rec
   // (host, nrec * (TARA_DIAG_VALUES + num_shells()) doubles)
@@ -147,6 +152,8 @@ struct SessionT : tara_session {
     drop_graphs();
     g.release(); u.release(); unew.release(); dold.release(); acc.release(); us.release(); us2.release();
     tmp.release(); dw.release();
+    if (rbuf) cudaFree(rbuf);
+    if (rstage) cudaFree(rstage);
     stage.release(); cw.release(); mw.release(); vw.release();
   }
 
@@ -447,6 +454,82 @@ struct SessionT : tara_session {
     return stepper == TARA_STEP_RK4 ? 4 * per : per;
   }
 
+  // real-space buffers: nf + 3 fields of Nx*Ny values, and FP64 staging
+  T* rbuf = nullptr;
+  double* rstage = nullptr;
+  int ensure_real() {
+    if (rbuf) return TARA_OK;
+    const size_t nn = (size_t)Nx * Ny;
+    if (cudaMalloc(&rbuf, (nf + 3) * nn * sizeof(T)) != cudaSuccess ||
+        cudaMalloc(&rstage, nn * sizeof(double)) != cudaSuccess) {
+      set_error("cudaMalloc of real-space buffers failed");
+      return TARA_ENOMEM;
+    }
+    return TARA_OK;
+  }
+  FieldPool<T>& workpool() { return model == TARA_MODEL_COH ? cw.H : model == TARA_MODEL_COM ? mw.H : vw.H; }
+  int real_fields(int what, double* const* h) override {
+    if (!h) { set_error("null field array"); return TARA_EINVAL; }
+    TARA_TRY(ensure_real());
+    const size_t nn = (size_t)Nx * Ny;
+    T* r[9];
+    for (int q = 0; q < nf + 3; q++) r[q] = rbuf + q * nn;
+    Cx<T>* st_[6];
+    Cx<T>* wk[8];
+    for (int q = 0; q < nf; q++) st_[q] = u[q];
+    // one work field per transformed field (pools hold >= nf, >= 4 fields)
+    const int nw = workpool().count < 8 ? workpool().count : 8;
+    for (int q = 0; q < 8; q++) wk[q] = q < nw ? workpool()[q] : nullptr;
+    if (nw < nf || nw < 3) { set_error("work pool too small"); return TARA_EINVAL; }
+    int nout = 0;
+    if (what == 0) {
+      TARA_TRY(state_to_real(g, nf, st_, r, wk, st));
+      nout = nf;
+    } else if (what == 1) {
+      Cx<T>* w3[3] = {tmp[0], tmp[1], model == TARA_MODEL_COM ? tmp[2] : wk[2]};
+      TARA_TRY(vorticity_real(g, model, st_, r[0], r + nf, w3, st));
+      nout = 1;
+    } else {
+      set_error("unknown real-space field set");
+      return TARA_EINVAL;
+    }
+    for (int q = 0; q < nout; q++) {
+      if (!h[q]) { set_error("null host field pointer"); return TARA_EINVAL; }
+      if constexpr (sizeof(T) == sizeof(double)) {
+        TARA_CUDA_TRY(cudaMemcpyAsync(h[q], r[q], nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+      } else {
+        copy_from_real(r[q], rstage, nn, st);
+        TARA_CUDA_TRY(cudaMemcpyAsync(h[q], rstage, nn * sizeof(double), cudaMemcpyDeviceToHost, st));
+      }
+      TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return device_status();
+  }
+  int set_state_real(const double* const* h) override {
+    if (!h) { set_error("null field array"); return TARA_EINVAL; }
+    TARA_TRY(ensure_real());
+    const size_t nn = (size_t)Nx * Ny;
+    const T* r[6];
+    Cx<T>* st_[6];
+    Cx<T>* wk[6];
+    for (int q = 0; q < nf; q++) {
+      if (!h[q]) { set_error("null host field pointer"); return TARA_EINVAL; }
+      T* d = rbuf + q * nn;
+      if constexpr (sizeof(T) == sizeof(double)) {
+        TARA_CUDA_TRY(cudaMemcpyAsync(d, h[q], nn * sizeof(double), cudaMemcpyHostToDevice, st));
+      } else {
+        TARA_CUDA_TRY(cudaMemcpyAsync(rstage, h[q], nn * sizeof(double), cudaMemcpyHostToDevice, st));
+        copy_to_real(rstage, d, nn, st);
+      }
+      r[q] = d;
+      st_[q] = u[q];
+      wk[q] = workpool()[q];
+    }
+    TARA_TRY(real_to_state(g, nf, r, st_, wk, st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return device_status();
+  }
+
   int num_shells() override { return diag_num_shells(Nx, Ny, p.Lx, p.Ly, p.pi); }
   int record(double* drec) {
     if (!dw.mem || dw.nbins != num_shells()) {
@@ -656,6 +739,64 @@ int tara_device_pci_bus_id(char* out, int len) {
 }
 
 int tara_launches_per_step(const tara_session* s, int stepper) { return s ? s->launches(stepper) : 0; }
+
+int tara_get_state_real(tara_session* s, double* const* fields) {
+  return s ? s->fail_if(s->real_fields(0, fields)) : TARA_EINVAL;
+}
+int tara_get_vorticity_real(tara_session* s, double* omega) {
+  if (!s || !omega) return TARA_EINVAL;
+  double* o[1] = {omega};
+  return s->fail_if(s->real_fields(1, o));
+}
+int tara_set_state_real(tara_session* s, const double* const* fields) {
+  return s ? s->fail_if(s->set_state_real(fields)) : TARA_EINVAL;
+}
+
+// The drivers' grid files: one line per grid point, x outer, y inner, as
+// list-directed records (src/main2com.f95:603-609: x, y, rho, ux, uy, P, E,
+// Bx, By; src/main2coh.f95:414-418: x, y, omega, n, ux, uy).
+int tara_write_snapshot(tara_session* s, const char* path) {
+  if (!s || !path) return TARA_EINVAL;
+  if (s->model != TARA_MODEL_COM && s->model != TARA_MODEL_COH) {
+    set_error("grid files are written for the hydro and MHD models");
+    return TARA_EUNSUPPORTED;
+  }
+  const size_t nn = (size_t)s->Nx * s->Ny;
+  std::vector<double> f((size_t)(s->nf + 1) * nn);
+  double* fp[7];
+  for (int q = 0; q <= s->nf; q++) fp[q] = f.data() + q * nn;
+  int r = s->real_fields(0, fp);
+  if (r == TARA_OK && s->model == TARA_MODEL_COH) r = s->real_fields(1, fp + s->nf);
+  if (r != TARA_OK) return s->fail_if(r);
+  FILE* out = std::fopen(path, "w");
+  if (!out) { set_error(std::string("cannot open ") + path); return TARA_EINVAL; }
+  const double dx = s->p.Lx / (double)s->Nx, dy = s->p.Ly / (double)s->Ny, cs2 = s->p.CS * s->p.CS;
+  std::string line;
+  double v[9];
+  for (int i = 0; i < s->Nx; i++)
+    for (int j = 0; j < s->Ny; j++) {
+      const size_t k = (size_t)j * s->Nx + i;
+      v[0] = 0.0 + (double)i * dx;
+      v[1] = 0.0 + (double)j * dy;
+      int n;
+      if (s->model == TARA_MODEL_COM) {
+        const double rho = fp[0][k];
+        v[2] = rho; v[3] = fp[1][k] / rho; v[4] = fp[2][k] / rho; v[5] = cs2 * rho;
+        v[6] = fp[3][k]; v[7] = fp[4][k]; v[8] = fp[5][k];
+        n = 9;
+      } else {
+        v[2] = fp[3][k]; v[3] = fp[0][k]; v[4] = fp[1][k]; v[5] = fp[2][k];
+        n = 6;
+      }
+      line.clear();
+      list_directed_append(line, v, n);
+      line += '\n';
+      std::fwrite(line.data(), 1, line.size(), out);
+    }
+  const bool ok = std::fclose(out) == 0;
+  if (!ok) { set_error(std::string("write to ") + path + " failed"); return TARA_EINVAL; }
+  return TARA_OK;
+}
 
 int tara_set_graphs(tara_session* s, int on) {
   if (!s) return TARA_EINVAL;
