@@ -136,6 +136,40 @@ int tara_set_state_real(tara_session* s, const double* const* fields);
 int tara_write_snapshot(tara_session* s, const char* path);
 int tara_format_list_directed(const double* v, int n, char* out, int cap);
 
+/* ---- learned subgrid closure of the MHD path (no counterpart in the
+ * reference) ----
+ * A CNN of four periodic 3x3 convolutions (5 -> 32 -> 32 -> 32 -> 4 channels,
+ * GELU after the first three; BF16 weights, FP32 activations and
+ * accumulation) maps the filtered coarse fields (rho - 1, ux, uy, Bx, By) on
+ * Nc x Nc to the subgrid stress (tau_xx, tau_xy, tau_yy) and EMF, each
+ * normalised by the channel means/scales of tara_closure_get_norm.
+ * Training pairs are made on the device from an FP64 MHD session on Nf x Nf
+ * (Nc divides Nf) by a sharp spectral filter:
+ *   tau_ij = filter(rho u_i u_j + B^2/2 d_ij - B_i B_j) - (same of the filtered state)
+ *   EMF    = filter(uy Bx - ux By) - (same of the filtered state).
+ * Attached to an FP64 MHD session on Nc x Nc, the RHS adds
+ * -(i kx tau_x. + i ky tau_.y) to the momentum and -i ky EMF / +i kx EMF to
+ * Bx / By, masked like the resolved fluxes.  Training and a coarse run must
+ * not overlap in time (they share the closure's buffers). */
+typedef struct tara_closure tara_closure;
+int tara_closure_open(tara_closure** out, int Nc, int capacity, int batch_max, unsigned long long seed);
+int tara_closure_close(tara_closure* c);
+int tara_closure_num_params(void);
+int tara_closure_count(const tara_closure* c);
+int tara_closure_add_pair(tara_closure* c, tara_session* fine);
+int tara_closure_get_pair(tara_closure* c, int idx, float* in5, float* out4);
+int tara_closure_get_norm(const tara_closure* c, float* norm18); /* mean_in[5] std_in[5] mean_out[4] std_out[4] */
+int tara_closure_set_norm(tara_closure* c, const float* norm18);
+int tara_closure_fit_norm(tara_closure* c, int first, int count);
+int tara_closure_train(tara_closure* c, int first, int count, int epochs, int batch, float lr, float* epoch_loss);
+int tara_closure_eval_loss(tara_closure* c, int first, int count, float* loss);
+int tara_closure_get_params(tara_closure* c, float* w);
+int tara_closure_set_params(tara_closure* c, const float* w);
+int tara_closure_forward(tara_closure* c, const float* in, int B, float* out);
+int tara_closure_backward(tara_closure* c, const float* in, const float* dout, int B, float* grad);
+int tara_session_attach_closure(tara_session* s, tara_closure* c); /* c = NULL detaches */
+int tara_filter_state(tara_session* fine, tara_session* coarse);
+
 /* ---- batched ensembles (no counterpart in the reference, whose drivers run
  * one grid per process) ----
  * n independent hydro (*2coh) runs, member m on an N[m] x N[m] grid

@@ -91,6 +91,22 @@ def lib():
         L.tara_device_pci_bus_id.argtypes = [C.c_char_p, I]
         L.tara_set_device.argtypes = [I]
         L.tara_set_graphs.argtypes = [P, I]
+        L.tara_closure_open.argtypes = [C.POINTER(C.c_void_p), I, I, I, C.c_ulonglong]
+        L.tara_closure_close.argtypes = [P]
+        L.tara_closure_count.argtypes = [P]
+        L.tara_closure_add_pair.argtypes = [P, P]
+        L.tara_closure_get_pair.argtypes = [P, I, P, P]
+        L.tara_closure_get_norm.argtypes = [P, P]
+        L.tara_closure_set_norm.argtypes = [P, P]
+        L.tara_closure_fit_norm.argtypes = [P, I, I]
+        L.tara_closure_train.argtypes = [P, I, I, I, I, C.c_float, P]
+        L.tara_closure_eval_loss.argtypes = [P, I, I, C.POINTER(C.c_float)]
+        L.tara_closure_get_params.argtypes = [P, P]
+        L.tara_closure_set_params.argtypes = [P, P]
+        L.tara_closure_forward.argtypes = [P, P, I, P]
+        L.tara_closure_backward.argtypes = [P, P, P, I, P]
+        L.tara_session_attach_closure.argtypes = [P, P]
+        L.tara_filter_state.argtypes = [P, P]
         L.tara_get_state_real.argtypes = [P, PP]
         L.tara_set_state_real.argtypes = [P, PP]
         L.tara_get_vorticity_real.argtypes = [P, P]
@@ -303,6 +319,113 @@ def _i32(v):
 
 def _d(v):
     return C.byref(C.c_double(v))
+
+
+class Closure:
+    """Learned subgrid closure (tara_closure_*): the CNN, its normalisation and
+    a device-resident dataset of (filtered fields, subgrid stress/EMF) pairs
+    on an Nc x Nc grid."""
+
+    def __init__(self, Nc: int, capacity: int, batch_max: int = 16, seed: int = 0):
+        self.Nc, self.capacity, self.batch_max = Nc, capacity, batch_max
+        h = C.c_void_p()
+        check(lib().tara_closure_open(C.byref(h), Nc, capacity, batch_max, seed), "tara_closure_open")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().tara_closure_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @staticmethod
+    def num_params() -> int:
+        return lib().tara_closure_num_params()
+
+    @property
+    def count(self) -> int:
+        return lib().tara_closure_count(self._h)
+
+    def add_pair(self, fine: "Session") -> None:
+        check(lib().tara_closure_add_pair(self._h, fine._h), "tara_closure_add_pair")
+
+    def get_pair(self, idx: int):
+        n = self.Nc
+        a = np.zeros((5, n, n), np.float32)
+        b = np.zeros((4, n, n), np.float32)
+        check(lib().tara_closure_get_pair(self._h, idx, a.ctypes.data, b.ctypes.data), "tara_closure_get_pair")
+        return a, b
+
+    def get_norm(self):
+        v = np.zeros(18, np.float32)
+        check(lib().tara_closure_get_norm(self._h, v.ctypes.data), "tara_closure_get_norm")
+        return v
+
+    def set_norm(self, v) -> None:
+        v = np.ascontiguousarray(v, dtype=np.float32)
+        assert v.size == 18
+        check(lib().tara_closure_set_norm(self._h, v.ctypes.data), "tara_closure_set_norm")
+
+    def fit_norm(self, first: int = 0, count: int = None) -> None:
+        count = self.count - first if count is None else count
+        check(lib().tara_closure_fit_norm(self._h, first, count), "tara_closure_fit_norm")
+
+    def train(self, first: int, count: int, epochs: int, batch: int = 8, lr: float = 1e-3):
+        losses = np.zeros(max(epochs, 1), np.float32)
+        check(lib().tara_closure_train(self._h, first, count, epochs, batch, C.c_float(lr), losses.ctypes.data),
+              "tara_closure_train")
+        return losses[:epochs]
+
+    def eval_loss(self, first: int, count: int) -> float:
+        v = C.c_float()
+        check(lib().tara_closure_eval_loss(self._h, first, count, C.byref(v)), "tara_closure_eval_loss")
+        return v.value
+
+    def get_params(self):
+        w = np.zeros(self.num_params(), np.float32)
+        check(lib().tara_closure_get_params(self._h, w.ctypes.data), "tara_closure_get_params")
+        return w
+
+    def set_params(self, w) -> None:
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        assert w.size == self.num_params()
+        check(lib().tara_closure_set_params(self._h, w.ctypes.data), "tara_closure_set_params")
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.zeros((x.shape[0], 4, self.Nc, self.Nc), np.float32)
+        check(lib().tara_closure_forward(self._h, x.ctypes.data, x.shape[0], out.ctypes.data), "tara_closure_forward")
+        return out
+
+    def backward(self, x, dout):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        dout = np.ascontiguousarray(dout, dtype=np.float32)
+        g = np.zeros(self.num_params(), np.float32)
+        check(lib().tara_closure_backward(self._h, x.ctypes.data, dout.ctypes.data, x.shape[0], g.ctypes.data),
+              "tara_closure_backward")
+        return g
+
+
+def attach_closure(session: "Session", closure) -> None:
+    """Add the closure's subgrid terms to the MHD RHS of `session` (None detaches)."""
+    check(lib().tara_session_attach_closure(session._h, closure._h if closure is not None else None),
+          "tara_session_attach_closure")
+
+
+def filter_state(fine: "Session", coarse: "Session") -> None:
+    """coarse state = sharp spectral filter of the fine state."""
+    check(lib().tara_filter_state(fine._h, coarse._h), "tara_filter_state")
 
 
 def format_list_directed(values) -> str:

@@ -8,9 +8,11 @@
 #include <tuple>
 #include <vector>
 #include "models.h"
+#include "closure.h"
 #include "diag.cuh"
 #include "output.h"
 #include "realspace.cuh"
+#include "session.h"
 
 using namespace tara;
 
@@ -88,50 +90,6 @@ int nfields_of(int model) {
 
 }  // namespace
 
-struct tara_session {
-  int model = 0, precision = 0, Nx = 0, Ny = 0, Nh = 0, nf = 0;
-  tara_params p{};
-  cudaStream_t st = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  int status = TARA_OK;
-  Prof prof;
-  virtual ~tara_session() {
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
-    if (st) cudaStreamDestroy(st);
-  }
-  virtual int init() = 0;
-  virtual int apply_params() = 0;
-  virtual int set_fields(int which, const double* const* h) = 0;  // which: 0 state, 1 history
-  virtual int get_fields(int which, double* const* h) = 0;
-  virtual int rhs_to_host(double* const* out) = 0;
-  virtual int step(int stepper, int n) = 0;
-  virtual int launches(int stepper) const = 0;
-  int fail_if(int s) {
-    if (s != TARA_OK && status == TARA_OK) status = s;
-    return s;
-  }
-  // Device status word: TARA_ETIMEOUT when a kernel's bounded wait ran out
-  // (the word is cleared after it has been reported).
-  virtual int device_status() = 0;
-  // elementwise stepper on host fields (drop-in ab2/euler/pc/rk4 entry points);
-  // nfld fields, each out = stepper(u, d1, d2)
-  virtual int elementwise(int mode, int nfld, const double* const* u, const double* const* d1,
-                          const double* const* d2, double* const* out) = 0;
-  // per-field PC / RK4 with the other hydro fields frozen (TARA_LEGACY_CORRECT)
-  virtual int frozen_field_step(bool rk4, int which, const double* const* f, const double* d,
-                                double* out) = 0;
-  virtual int num_shells() = 0;
-  virtual void set_graphs(bool on) = 0;
-  // what = 0: the nf state fields in real space (c2r / NxNy); 1: vorticity
-  virtual int real_fields(int what, double* const* h) = 0;
-  virtual int set_state_real(const double* const* h) = 0;
-  // nrec diagnostics records of the state, one before the first step and one
-  // after every `every` steps (nsteps = (nrec - 1) * every), into rec
-  // (host, nrec * (TARA_DIAG_VALUES + num_shells()) doubles)
-  virtual int run_recorded(int stepper, int every, int nrec, double* rec) = 0;
-};
-
 namespace {
 
 template <class T>
@@ -151,7 +109,7 @@ struct SessionT : tara_session {
     if (st) cudaStreamSynchronize(st);
     drop_graphs();
     g.release(); u.release(); unew.release(); dold.release(); acc.release(); us.release(); us2.release();
-    tmp.release(); dw.release();
+    tmp.release(); dw.release(); closf.release();
     if (rbuf) cudaFree(rbuf);
     if (rstage) cudaFree(rstage);
     stage.release(); cw.release(); mw.release(); vw.release();
@@ -273,9 +231,39 @@ struct SessionT : tara_session {
   int rhs(Cx<T>* const* in, const StepArgs<T>& s) {
     switch (model) {
       case TARA_MODEL_COH: return coh_rhs(g, cw, cohp, in, s, st);
-      case TARA_MODEL_COM: return com_rhs(g, mw, comp, in, s, st);
+      case TARA_MODEL_COM:
+        if constexpr (sizeof(T) == sizeof(double)) {
+          if (clos) {  // the learned closure's stress/EMF spectra for this RHS input
+            Cx<double>* out4[4] = {closf[0], closf[1], closf[2], closf[3]};
+            TARA_TRY(closure_terms(clos, g, in, out4, st));
+          }
+        }
+        return com_rhs(g, mw, comp, in, s, st);
       default: return vort_rhs(g, vw, vortp, in, s, st);
     }
+  }
+
+  // learned closure (MHD, FP64 sessions of the closure's coarse grid)
+  tara_closure* clos = nullptr;
+  FieldPool<T> closf;
+  const void* grid_ptr() const override { return &g; }
+  void* state_ptr(int q) override { return q >= 0 && q < nf ? (void*)u[q] : nullptr; }
+  int attach_closure(tara_closure* c) override {
+    drop_graphs();
+    if (!c) {
+      clos = nullptr;
+      comp.closure = 0;
+      return TARA_OK;
+    }
+    if (model != TARA_MODEL_COM || sizeof(T) != sizeof(double) || Nx != Ny || Nx != closure_grid(c)) {
+      set_error("a closure attaches to an FP64 MHD session on its coarse grid");
+      return TARA_EINVAL;
+    }
+    if (!closf.base) TARA_TRY(closf.alloc(g, 4, st));
+    clos = c;
+    comp.closure = 1;
+    for (int q = 0; q < 4; q++) comp.clos[q] = closf[q];
+    return TARA_OK;
   }
   StepArgs<T> base_args(int mode) {
     StepArgs<T> s{};

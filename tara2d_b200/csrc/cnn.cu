@@ -1,0 +1,327 @@
+// Closure CNN kernels and their host driver (see cnn.cuh).
+//
+//   k_conv      3x3 periodic convolution of a 16x16 pixel tile for every
+//               output channel: the input tile with its one-pixel halo
+//               (wrapped around the periodic box) and the layer's weights
+//               (BF16, widened to FP32) are staged in shared memory; each
+//               thread accumulates one pixel's COUT outputs in FP32.  The
+//               epilogue adds the bias and applies GELU (keeping the
+//               pre-activation), nothing, or the GELU derivative of the
+//               previous layer (input-gradient pass with mirrored weights).
+//   k_conv_dw   weight and bias gradients of one tile: each thread owns
+//               (cout, cin) pairs and all 9 taps; per-CTA partials are then
+//               summed in a fixed order by k_sum_parts.
+//   k_mse, k_adam, k_pack_weights: loss/gradient, optimiser, BF16 layouts.
+#include <cmath>
+#include <cstring>
+#include "cnn.cuh"
+#include "plan.h"
+
+namespace tara {
+
+namespace {
+
+constexpr int kTile = 16, kHalo = 18, kPlane = kHalo * kHalo;
+
+enum { EPI_GELU = 0, EPI_LINEAR = 1, EPI_GELUGRAD = 2 };
+
+__device__ __forceinline__ float gelu(float v) { return 0.5f * v * (1.0f + erff(v * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float v) {
+  return 0.5f * (1.0f + erff(v * 0.70710678118654752f)) + v * 0.39894228040143268f * expf(-0.5f * v * v);
+}
+
+__device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+template <int CIN, int COUT, int EPI>
+__global__ void __launch_bounds__(256) k_conv(const float* __restrict__ in, const __nv_bfloat16* __restrict__ w,
+                                              const float* __restrict__ bias, float* __restrict__ z,
+                                              float* __restrict__ out, const float* __restrict__ zprev, int H,
+                                              int W) {
+  static_assert(COUT % 4 == 0, "output channels in groups of four");
+  extern __shared__ __align__(16) float sm[];
+  float* xs = sm;                  // [CIN][18][18]
+  float* ws = sm + CIN * kPlane;   // [CIN*9][COUT]
+  const int b = blockIdx.z, y0 = blockIdx.y * kTile, x0 = blockIdx.x * kTile;
+  const int tid = threadIdx.x, ty = tid / kTile, tx = tid % kTile;
+  const size_t plane = (size_t)H * W;
+  const float* inb = in + (size_t)b * CIN * plane;
+  for (int q = tid; q < CIN * kPlane; q += 256) {
+    const int c = q / kPlane, r = q % kPlane;
+    const int gy = wrap(y0 + r / kHalo - 1, H), gx = wrap(x0 + r % kHalo - 1, W);
+    xs[q] = __ldg(inb + c * plane + (size_t)gy * W + gx);
+  }
+  for (int q = tid; q < CIN * 9 * COUT; q += 256) ws[q] = __bfloat162float(w[q]);
+  __syncthreads();
+  float acc[COUT];
+#pragma unroll
+  for (int co = 0; co < COUT; co++) acc[co] = 0.0f;
+#pragma unroll 1
+  for (int ci = 0; ci < CIN; ci++) {
+#pragma unroll
+    for (int tap = 0; tap < 9; tap++) {
+      const float xv = xs[ci * kPlane + (ty + tap / 3) * kHalo + tx + tap % 3];
+      const float4* wr = reinterpret_cast<const float4*>(ws + (ci * 9 + tap) * COUT);
+#pragma unroll
+      for (int k = 0; k < COUT / 4; k++) {
+        const float4 w4 = wr[k];
+        acc[4 * k] = fmaf(xv, w4.x, acc[4 * k]);
+        acc[4 * k + 1] = fmaf(xv, w4.y, acc[4 * k + 1]);
+        acc[4 * k + 2] = fmaf(xv, w4.z, acc[4 * k + 2]);
+        acc[4 * k + 3] = fmaf(xv, w4.w, acc[4 * k + 3]);
+      }
+    }
+  }
+  const size_t po = (size_t)(y0 + ty) * W + x0 + tx;
+#pragma unroll
+  for (int co = 0; co < COUT; co++) {
+    const float v = acc[co] + (bias ? __ldg(bias + co) : 0.0f);
+    const size_t idx = ((size_t)b * COUT + co) * plane + po;
+    if constexpr (EPI == EPI_GELU) {
+      z[idx] = v;
+      out[idx] = gelu(v);
+    } else if constexpr (EPI == EPI_LINEAR) {
+      out[idx] = v;
+    } else {
+      out[idx] = v * gelu_d(__ldg(zprev + idx));
+    }
+  }
+}
+
+// weight (and bias) gradient partials of one 16x16 tile of one sample
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(256) k_conv_dw(const float* __restrict__ in, const float* __restrict__ dz,
+                                                 float* __restrict__ part, int H, int W) {
+  constexpr int XS = kPlane + 1;  // odd plane stride: lanes with consecutive cin hit distinct banks
+  constexpr int NP = COUT * CIN, NPT = (NP + 255) / 256, NWL = COUT * CIN * 9 + COUT;
+  extern __shared__ __align__(16) float sm[];
+  float* xs = sm;              // [CIN][18*18 + 1]
+  float* ds = sm + CIN * XS;   // [COUT][256]
+  const int b = blockIdx.z, y0 = blockIdx.y * kTile, x0 = blockIdx.x * kTile;
+  const int tid = threadIdx.x;
+  const size_t plane = (size_t)H * W;
+  for (int q = tid; q < CIN * kPlane; q += 256) {
+    const int c = q / kPlane, r = q % kPlane;
+    const int gy = wrap(y0 + r / kHalo - 1, H), gx = wrap(x0 + r % kHalo - 1, W);
+    xs[c * XS + r] = __ldg(in + ((size_t)b * CIN + c) * plane + (size_t)gy * W + gx);
+  }
+  for (int q = tid; q < COUT * 256; q += 256) {
+    const int c = q / 256, p = q % 256;
+    ds[q] = __ldg(dz + ((size_t)b * COUT + c) * plane + (size_t)(y0 + p / kTile) * W + x0 + p % kTile);
+  }
+  __syncthreads();
+  float acc[NPT][9];
+#pragma unroll
+  for (int k = 0; k < NPT; k++)
+#pragma unroll
+    for (int t = 0; t < 9; t++) acc[k][t] = 0.0f;
+#pragma unroll 1
+  for (int p = 0; p < 256; p++) {
+    const int py = p / kTile, px = p % kTile;
+#pragma unroll
+    for (int k = 0; k < NPT; k++) {
+      const int q = tid + k * 256;
+      if (q < NP) {
+        const int co = q / CIN, ci = q % CIN;
+        const float d = ds[co * 256 + p];
+        const float* xb = xs + ci * XS + py * kHalo + px;
+#pragma unroll
+        for (int t = 0; t < 9; t++) acc[k][t] = fmaf(d, xb[(t / 3) * kHalo + t % 3], acc[k][t]);
+      }
+    }
+  }
+  const size_t cta = ((size_t)b * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  float* pp = part + cta * NWL;
+#pragma unroll
+  for (int k = 0; k < NPT; k++) {
+    const int q = tid + k * 256;
+    if (q < NP)
+#pragma unroll
+      for (int t = 0; t < 9; t++) pp[q * 9 + t] = acc[k][t];  // (co*CIN + ci)*9 + tap
+  }
+  if (tid < COUT) {
+    float s = 0.0f;
+    for (int p = 0; p < 256; p++) s += ds[tid * 256 + p];
+    pp[COUT * CIN * 9 + tid] = s;
+  }
+}
+
+__global__ void k_sum_parts(const float* __restrict__ part, int nct, int nw, float* __restrict__ g) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int c = 0; c < nct; c++) s += part[(size_t)c * nw + i];
+    g[i] = s;
+  }
+}
+
+// master W[cout][cin][3][3], b[cout] -> BF16 [cin][9][cout] and mirrored
+// [cout][9][cin]; bias rounded to BF16 (kept as FP32)
+__global__ void k_pack_weights(const float* __restrict__ m, int cin, int cout, __nv_bfloat16* wf,
+                               __nv_bfloat16* wb, float* bias) {
+  const int nw = cout * cin * 9;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw + cout; i += gridDim.x * blockDim.x) {
+    if (i < nw) {
+      const int co = i / (cin * 9), ci = (i / 9) % cin, tap = i % 9;
+      const __nv_bfloat16 v = __float2bfloat16_rn(m[i]);
+      wf[(ci * 9 + tap) * cout + co] = v;
+      wb[(co * 9 + (8 - tap)) * cin + ci] = v;
+    } else {
+      bias[i] = __bfloat162float(__float2bfloat16_rn(m[i]));  // same offset as in the master vector
+    }
+  }
+}
+
+__global__ void k_mse(const float* __restrict__ o, const float* __restrict__ t, size_t n, float* __restrict__ d,
+                      double* __restrict__ acc) {
+  __shared__ double red[8];
+  double s = 0.0;
+  const float sc = 2.0f / (float)n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float e = o[i] - t[i];
+    d[i] = sc * e;
+    s += (double)e * e;
+  }
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x / 32); w++) r += red[w];
+    atomicAdd(acc, r);
+  }
+}
+
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+int layer_params(int l) {
+  const CnnLayerDims d = cnn_layer(l);
+  return d.cout * d.cin * 9 + d.cout;
+}
+int layer_offset(int l) {
+  int o = 0;
+  for (int k = 0; k < l; k++) o += layer_params(k);
+  return o;
+}
+
+template <int CIN, int COUT, int EPI>
+void launch_conv(const float* in, const __nv_bfloat16* w, const float* bias, float* z, float* out,
+                 const float* zprev, int B, int H, int W, cudaStream_t st) {
+  const size_t smem = (size_t)(CIN * kPlane + CIN * 9 * COUT) * sizeof(float);
+  auto kern = k_conv<CIN, COUT, EPI>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<dim3(W / kTile, H / kTile, B), 256, smem, st>>>(in, w, bias, z, out, zprev, H, W);
+}
+template <int CIN, int COUT>
+void launch_dw(const float* in, const float* dz, float* part, float* g, int B, int H, int W, cudaStream_t st) {
+  const size_t smem = (size_t)(CIN * (kPlane + 1) + COUT * 256) * sizeof(float);
+  auto kern = k_conv_dw<CIN, COUT>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<dim3(W / kTile, H / kTile, B), 256, smem, st>>>(in, dz, part, H, W);
+  const int nct = B * (H / kTile) * (W / kTile), nw = COUT * CIN * 9 + COUT;
+  k_sum_parts<<<(nw + 255) / 256, 256, 0, st>>>(part, nct, nw, g);
+}
+
+}  // namespace
+
+int cnn_num_params() { return layer_offset(kCnnLayers); }
+
+int Cnn::alloc(int H_, int W_, int Bmax_) {
+  if (H_ % kTile || W_ % kTile || H_ < kTile || W_ < kTile || Bmax_ < 1) {
+    set_error("CNN planes must be multiples of 16");
+    return TARA_EINVAL;
+  }
+  H = H_; W = W_; Bmax = Bmax_;
+  const size_t np = cnn_num_params(), plane = (size_t)H * W;
+  auto am = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess; };
+  bool ok = am((void**)&master, np * 4) && am((void**)&grad, np * 4) && am((void**)&adam_m, np * 4) &&
+            am((void**)&adam_v, np * 4) && am((void**)&biasbuf, np * 4) && am((void**)&lossacc, sizeof(double));
+  for (int l = 0; l < kCnnLayers && ok; l++) {
+    const CnnLayerDims d = cnn_layer(l);
+    ok = am((void**)&wfwd[l], (size_t)d.cin * 9 * d.cout * 2) && am((void**)&wbwd[l], (size_t)d.cin * 9 * d.cout * 2);
+    if (ok && d.gelu) ok = am((void**)&z[l], (size_t)Bmax * d.cout * plane * 4);
+    if (ok) ok = am((void**)&a[l], (size_t)Bmax * d.cout * plane * 4);
+    bias[l] = biasbuf + layer_offset(l) + d.cout * d.cin * 9;
+  }
+  for (int k = 0; k < 2 && ok; k++) ok = am((void**)&dz[k], (size_t)Bmax * kCnnHid * plane * 4);
+  part_elems = (size_t)Bmax * (H / kTile) * (W / kTile) * (kCnnHid * kCnnHid * 9 + kCnnHid);
+  if (ok) ok = am((void**)&part, part_elems * 4);
+  if (!ok) {
+    set_error("cudaMalloc of CNN buffers failed");
+    return TARA_ENOMEM;
+  }
+  cudaMemset(adam_m, 0, np * 4);
+  cudaMemset(adam_v, 0, np * 4);
+  return TARA_OK;
+}
+
+void Cnn::release() {
+  for (void* p : {(void*)master, (void*)grad, (void*)adam_m, (void*)adam_v, (void*)biasbuf, (void*)lossacc,
+                  (void*)part, (void*)dz[0], (void*)dz[1]})
+    if (p) cudaFree(p);
+  for (int l = 0; l < kCnnLayers; l++)
+    for (void* p : {(void*)wfwd[l], (void*)wbwd[l], (void*)z[l], (void*)a[l]})
+      if (p) cudaFree(p);
+  *this = Cnn{};
+}
+
+int Cnn::refresh(cudaStream_t st) {
+  for (int l = 0; l < kCnnLayers; l++) {
+    const CnnLayerDims d = cnn_layer(l);
+    k_pack_weights<<<64, 256, 0, st>>>(master + layer_offset(l), d.cin, d.cout, wfwd[l], wbwd[l],
+                                       biasbuf + layer_offset(l));
+  }
+  TARA_CUDA_TRY(cudaGetLastError());
+  return TARA_OK;
+}
+
+int Cnn::forward(const float* in, int B, bool, cudaStream_t st) {
+  if (B < 1 || B > Bmax) { set_error("batch larger than the CNN buffers"); return TARA_EINVAL; }
+  launch_conv<kCnnIn, kCnnHid, EPI_GELU>(in, wfwd[0], bias[0], z[0], a[0], nullptr, B, H, W, st);
+  launch_conv<kCnnHid, kCnnHid, EPI_GELU>(a[0], wfwd[1], bias[1], z[1], a[1], nullptr, B, H, W, st);
+  launch_conv<kCnnHid, kCnnHid, EPI_GELU>(a[1], wfwd[2], bias[2], z[2], a[2], nullptr, B, H, W, st);
+  launch_conv<kCnnHid, kCnnOut, EPI_LINEAR>(a[2], wfwd[3], bias[3], nullptr, a[3], nullptr, B, H, W, st);
+  TARA_CUDA_TRY(cudaGetLastError());
+  return TARA_OK;
+}
+
+int Cnn::backward(const float* in, const float* dout, int B, cudaStream_t st) {
+  if (B < 1 || B > Bmax) { set_error("batch larger than the CNN buffers"); return TARA_EINVAL; }
+  // layer 3 (linear): dout is the gradient of its pre-activation
+  launch_dw<kCnnHid, kCnnOut>(a[2], dout, part, grad + layer_offset(3), B, H, W, st);
+  launch_conv<kCnnOut, kCnnHid, EPI_GELUGRAD>(dout, wbwd[3], nullptr, nullptr, dz[0], z[2], B, H, W, st);
+  launch_dw<kCnnHid, kCnnHid>(a[1], dz[0], part, grad + layer_offset(2), B, H, W, st);
+  launch_conv<kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[0], wbwd[2], nullptr, nullptr, dz[1], z[1], B, H, W, st);
+  launch_dw<kCnnHid, kCnnHid>(a[0], dz[1], part, grad + layer_offset(1), B, H, W, st);
+  launch_conv<kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[1], wbwd[1], nullptr, nullptr, dz[0], z[0], B, H, W, st);
+  launch_dw<kCnnIn, kCnnHid>(in, dz[0], part, grad + layer_offset(0), B, H, W, st);
+  TARA_CUDA_TRY(cudaGetLastError());
+  return TARA_OK;
+}
+
+int Cnn::mse(const float* target, int B, cudaStream_t st) {
+  const size_t n = (size_t)B * kCnnOut * H * W;
+  k_mse<<<296, 256, 0, st>>>(a[3], target, n, dz[1], lossacc);
+  TARA_CUDA_TRY(cudaGetLastError());
+  return TARA_OK;
+}
+
+int Cnn::adam(float lr, float b1, float b2, float eps, cudaStream_t st) {
+  adam_t++;
+  const float c1 = 1.0f - (float)std::pow((double)b1, (double)adam_t);
+  const float c2 = 1.0f - (float)std::pow((double)b2, (double)adam_t);
+  const int n = cnn_num_params();
+  k_adam<<<(n + 255) / 256, 256, 0, st>>>(master, grad, adam_m, adam_v, n, lr, b1, b2, eps, c1, c2);
+  TARA_CUDA_TRY(cudaGetLastError());
+  return refresh(st);
+}
+
+}  // namespace tara

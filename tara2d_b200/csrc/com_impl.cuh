@@ -283,6 +283,8 @@ template <class T> struct ColFwdComArgs {
   const Cx<T>* in[6];  // stage input (the state the RHS is evaluated at)
   T mu, eta;
   int forcing;
+  int closure;            // add the subgrid stress / EMF spectra of clos[]
+  const Cx<T>* clos[4];   // tau_xx, tau_xy, tau_yy, EMF
   StepArgs<T> step;
 };
 
@@ -347,6 +349,14 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_c
         fft(a.X[f == 1 ? XFX : XFY]);
         each([&](int q, int, int, bool) { d[q] = d[q] + v[q]; });
       }
+      if (a.closure) {  // -(i kx tau_x. + i ky tau_.y), masked like the fluxes
+        const Cx<T>* ta = a.clos[f == 1 ? 0 : 1];
+        const Cx<T>* tb = a.clos[f == 1 ? 1 : 2];
+        each([&](int q, int c, int j, bool m) {
+          const size_t o = (size_t)j * ld + c;
+          if (!m) d[q] = d[q] - (ikmul(__ldg(kx + c), ldg(ta + o)) + ikmul(__ldg(ky + j), ldg(tb + o)));
+        });
+      }
       break;
     case 3:  // -(i kx Ex + i ky Ey) + mu E_Visc_k                          (:412-413)
       fft(a.X[XEX]);
@@ -367,6 +377,10 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_c
         const Cx<T> p = m ? zero : rmul(k1 * k1, B);
         const Cx<T> s = m ? zero : rmul(k2 * k2, B);
         d[q] = -nl - rmul(eta, p + s);
+        if (a.closure && !m) {  // subgrid EMF: -i ky EMF (Bx), +i kx EMF (By)
+          const Cx<T> e = ldg(a.clos[3] + o);
+          d[q] = f == 4 ? d[q] - ikmul(k2, e) : d[q] + ikmul(k1, e);
+        }
       });
       break;
   }
@@ -505,6 +519,8 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   cf.mu = p.mu;
   cf.eta = p.eta;
   cf.forcing = forcing;
+  cf.closure = p.closure;
+  for (int q = 0; q < 4; q++) cf.clos[q] = p.clos[q];
   cf.step = step;
   prof_mark(g.prof, st, KK_COL_FWD_COM);
   TARA_DISPATCH_LEN(g.Ny, col_fwd_com_dispatch, cf, st)

@@ -25,7 +25,14 @@ int coh_rhs(const Grid<T>& g, CohWork<T>& w, const CohParamsT<T>& p, Cx<T>* cons
 constexpr int kCohLaunches = 3;
 
 // ---- compressible MHD, src/derive2com.f95 ----
-template <class T> struct ComParamsT { T mu, eta, cs2, kf, A; int fix_curlB; };
+// closure != 0: the spectra of a subgrid stress (xx, xy, yy) and EMF in
+// clos[] are added to the momentum and induction fluxes (learned closure).
+template <class T> struct ComParamsT {
+  T mu, eta, cs2, kf, A;
+  int fix_curlB;
+  int closure;
+  const Cx<T>* clos[4];
+};
 template <class T> struct ComWork {
   FieldPool<T> H;  // half-real: rho, rho_ux, rho_uy, E, Bx, By, d(uy)/dy, [iky Bx, ikx By]
   FieldPool<T> X;  // x-transformed rows: ux, uy, Mxx, Mxy, Myy, Mag, Ex, Ey, EV, Fx, Fy
