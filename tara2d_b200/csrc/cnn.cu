@@ -32,16 +32,20 @@ __device__ __forceinline__ float gelu_d(float v) {
 
 __device__ __forceinline__ int wrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
-template <int CIN, int COUT, int EPI>
+// COUTT output channels in all, COUT of them (from blockIdx.z % (COUTT/COUT))
+// per CTA: small batches split the channels over more CTAs.
+template <int CIN, int COUTT, int COUT, int EPI>
 __global__ void __launch_bounds__(256) k_conv(const float* __restrict__ in, const __nv_bfloat16* __restrict__ w,
                                               const float* __restrict__ bias, float* __restrict__ z,
                                               float* __restrict__ out, const float* __restrict__ zprev, int H,
                                               int W) {
-  static_assert(COUT % 4 == 0, "output channels in groups of four");
+  static_assert(COUT % 4 == 0 && COUTT % COUT == 0, "output channels in groups of four");
+  constexpr int S = COUTT / COUT;
   extern __shared__ __align__(16) float sm[];
   float* xs = sm;                  // [CIN][18][18]
   float* ws = sm + CIN * kPlane;   // [CIN*9][COUT]
-  const int b = blockIdx.z, y0 = blockIdx.y * kTile, x0 = blockIdx.x * kTile;
+  const int b = blockIdx.z / S, c0 = (blockIdx.z % S) * COUT;
+  const int y0 = blockIdx.y * kTile, x0 = blockIdx.x * kTile;
   const int tid = threadIdx.x, ty = tid / kTile, tx = tid % kTile;
   const size_t plane = (size_t)H * W;
   const float* inb = in + (size_t)b * CIN * plane;
@@ -50,7 +54,7 @@ __global__ void __launch_bounds__(256) k_conv(const float* __restrict__ in, cons
     const int gy = wrap(y0 + r / kHalo - 1, H), gx = wrap(x0 + r % kHalo - 1, W);
     xs[q] = __ldg(inb + c * plane + (size_t)gy * W + gx);
   }
-  for (int q = tid; q < CIN * 9 * COUT; q += 256) ws[q] = __bfloat162float(w[q]);
+  for (int q = tid; q < CIN * 9 * COUT; q += 256) ws[q] = __bfloat162float(w[(q / COUT) * COUTT + c0 + q % COUT]);
   __syncthreads();
   float acc[COUT];
 #pragma unroll
@@ -74,8 +78,8 @@ __global__ void __launch_bounds__(256) k_conv(const float* __restrict__ in, cons
   const size_t po = (size_t)(y0 + ty) * W + x0 + tx;
 #pragma unroll
   for (int co = 0; co < COUT; co++) {
-    const float v = acc[co] + (bias ? __ldg(bias + co) : 0.0f);
-    const size_t idx = ((size_t)b * COUT + co) * plane + po;
+    const float v = acc[co] + (bias ? __ldg(bias + c0 + co) : 0.0f);
+    const size_t idx = ((size_t)b * COUTT + c0 + co) * plane + po;
     if constexpr (EPI == EPI_GELU) {
       z[idx] = v;
       out[idx] = gelu(v);
@@ -212,13 +216,26 @@ int layer_offset(int l) {
   return o;
 }
 
+template <int CIN, int COUTT, int COUT, int EPI>
+void launch_conv_split(const float* in, const __nv_bfloat16* w, const float* bias, float* z, float* out,
+                       const float* zprev, int B, int H, int W, cudaStream_t st) {
+  const size_t smem = (size_t)(CIN * kPlane + CIN * 9 * COUT) * sizeof(float);
+  auto kern = k_conv<CIN, COUTT, COUT, EPI>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<dim3(W / kTile, H / kTile, B * (COUTT / COUT)), 256, smem, st>>>(in, w, bias, z, out, zprev, H, W);
+}
+// fewer than ~4 tiles per SM: a quarter of the output channels per CTA
 template <int CIN, int COUT, int EPI>
 void launch_conv(const float* in, const __nv_bfloat16* w, const float* bias, float* z, float* out,
                  const float* zprev, int B, int H, int W, cudaStream_t st) {
-  const size_t smem = (size_t)(CIN * kPlane + CIN * 9 * COUT) * sizeof(float);
-  auto kern = k_conv<CIN, COUT, EPI>;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  kern<<<dim3(W / kTile, H / kTile, B), 256, smem, st>>>(in, w, bias, z, out, zprev, H, W);
+  const int tiles = B * (H / kTile) * (W / kTile);
+  if constexpr (COUT == kCnnHid) {
+    if (tiles < 600) {
+      launch_conv_split<CIN, COUT, COUT / 4, EPI>(in, w, bias, z, out, zprev, B, H, W, st);
+      return;
+    }
+  }
+  launch_conv_split<CIN, COUT, COUT, EPI>(in, w, bias, z, out, zprev, B, H, W, st);
 }
 template <int CIN, int COUT>
 void launch_dw(const float* in, const float* dz, float* part, float* g, int B, int H, int W, cudaStream_t st) {
