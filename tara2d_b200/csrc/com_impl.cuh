@@ -384,15 +384,13 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_c
       });
       break;
   }
-#pragma unroll
-  for (int q = 0; q < P / RL; q++)
-#pragma unroll
-    for (int r = 0; r < RL; r++) {
-      int t, i;
-      F::template out_pos<F::S - 1>(tid, q, r, t, i);
-      const int c = c0 + t;
-      if (c < Nh) step_apply(a.step, f, (size_t)i * ld + c, d[q * RL + r]);
-    }
+  step_apply_n<T, P>(a.step, f, [&](int e, size_t& idx) {
+    int t, i;
+    F::template out_pos<F::S - 1>(tid, e / RL, e % RL, t, i);
+    const int c = c0 + t;
+    idx = (size_t)i * ld + c;
+    return c < Nh;
+  }, d);
 }
 
 template <int L, class T>

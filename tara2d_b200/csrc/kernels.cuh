@@ -278,6 +278,61 @@ __device__ __forceinline__ void step_apply(const StepArgs<T>& s, int f, size_t i
   }
 }
 
+// The update of step_apply for the N elements a thread holds: every load is
+// issued before the first store.  Element by element, each element's loads
+// would wait for the previous element's stores (the compiler cannot tell that
+// they never alias), so a thread would wait on memory N times in a row.
+// pos(e, idx) gives element e's index and whether it exists.  Same
+// arithmetic as step_apply, element for element.
+template <class T, int N, class POS>
+__device__ __forceinline__ void step_apply_n(const StepArgs<T>& s, int f, POS&& pos, const Cx<T>* d) {
+  if (s.mode == STEP_RHS) {
+#pragma unroll
+    for (int e = 0; e < N; e++) {
+      size_t idx;
+      if (pos(e, idx)) st(s.out[f] + idx, d[e]);
+    }
+    return;
+  }
+  const bool rk4 = s.mode == STEP_RK4;
+  const bool need0 = s.mode == STEP_AB2 || (rk4 && s.stage > 0);  // AB2 history or RK4 accumulator
+  const bool need1 = !rk4 || s.stage < 3;                          // state
+  const Cx<T>* p0 = s.mode == STEP_AB2 ? s.dold[f] : s.acc[f];
+  const Cx<T>* p1 = s.u[f];
+  Cx<T> x0[N], x1[N];
+#pragma unroll
+  for (int e = 0; e < N; e++) {
+    size_t idx;
+    x0[e] = x1[e] = cx<T>(0, 0);
+    if (pos(e, idx)) {
+      if (need0) x0[e] = ld(p0 + idx);
+      if (need1) x1[e] = ld(p1 + idx);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < N; e++) {
+    size_t idx;
+    if (!pos(e, idx)) continue;
+    const Cx<T> de = d[e];
+    if (s.mode == STEP_AB2) {
+      const Cx<T> inc = rmul((T)1.5, de) - rmul((T)0.5, x0[e]);
+      st(s.unew[f] + idx, x1[e] + rmul(s.dt, inc));
+      st(s.dold[f] + idx, de);
+    } else if (s.mode == STEP_EULER) {
+      st(s.unew[f] + idx, x1[e] + rmul(s.dt, de));
+      st(s.dold[f] + idx, de);
+    } else if (s.stage == 0) {
+      st(s.acc[f] + idx, x1[e] + rmul(s.wa, de));
+      st(s.us[f] + idx, x1[e] + rmul(s.cs, de));
+    } else if (s.stage < 3) {
+      st(s.acc[f] + idx, x0[e] + rmul(s.wa, de));
+      st(s.us[f] + idx, x1[e] + rmul(s.cs, de));
+    } else {
+      st(s.unew[f] + idx, x0[e] + rmul(s.wa, de));
+    }
+  }
+}
+
 // ------------------------------------------------------------ forward y pass
 // One output field per CTA row of the grid (blockIdx.y = f): forward y DFT of
 // X[f], circular 2/3 dealiasing, sign, then the stepper update.
@@ -303,14 +358,24 @@ __device__ __forceinline__ void col_fwd_simple_tile(const ColFwdSimpleArgs<T>& a
     return ldg(X + (size_t)i * ld + c);
   }, SyncBlock{});
   const T sg = a.sign[f];
-  fft_emit<F>(tid, v, [&](int t, int j, Cx<T> x) {
-    const int c = c0 + t;
-    if (c >= Nh) return;
+  constexpr int RL = F::Pl::R[F::S - 1];
+  // derivative values in the order fft_emit visits them: element e = q*RL + r
+#pragma unroll
+  for (int e = 0; e < P; e++) {
+    int t, j;
+    F::template out_pos<F::S - 1>(tid, e / RL, e % RL, t, j);
+    const int c = min(c0 + t, Nh - 1);
     const bool masked = !a.nomask && c >= __ldg(a.tb.cut + j);
-    Cx<T> val = masked ? cx<T>(0, 0) : x;
-    Cx<T> d = cx<T>(sg * val.x, sg * val.y);
-    step_apply(a.step, f, (size_t)j * ld + c, d);
-  });
+    const Cx<T> val = masked ? cx<T>(0, 0) : v[e];
+    v[e] = cx<T>(sg * val.x, sg * val.y);
+  }
+  step_apply_n<T, P>(a.step, f, [&](int e, size_t& idx) {
+    int t, j;
+    F::template out_pos<F::S - 1>(tid, e / RL, e % RL, t, j);
+    const int c = c0 + t;
+    idx = (size_t)j * ld + c;
+    return c < Nh;
+  }, v);
 }
 
 template <class T, int L, int CB, int P>
