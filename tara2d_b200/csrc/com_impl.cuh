@@ -25,7 +25,9 @@
 
 namespace tara {
 
-enum : int { XUX = 0, XUY, XMXX, XMXY, XMYY, XMAG, XEX, XEY, XEV, XFX, XFY };
+// XEX2/XEY2: the curl-B parts of the energy fluxes (second row pass), added
+// to XEX/XEY as the column pass loads them
+enum : int { XUX = 0, XUY, XMXX, XMXY, XMYY, XMAG, XEX, XEY, XEV, XFX, XFY, XEX2, XEY2 };
 enum : int { HRHO = 0, HMX, HMY, HE, HBX, HBY, HDUY, HIKYBX };
 
 // Rows per CTA so that a CTA has at least ~128 threads, within the shared
@@ -187,8 +189,8 @@ template <class T> struct RowCom2Args {
   const Cx<T>* Hbx;
   const Cx<T>* Hby;
   const Cx<T>* Hikybx;
-  Cx<T>* Xex;
-  Cx<T>* Xey;
+  Cx<T>* Xex2;  // written, not updated: the column pass adds them to Ex, Ey
+  Cx<T>* Xey2;
   Cx<T>* Xev;
   T eta, inv_nx;
   int rb;
@@ -269,17 +271,15 @@ k_row_com2(const RowCom2Args<T> a) {
   __syncthreads();  // inputs gathered: arrays 0..2 become exchange buffers
   if (th.g < 3) {
     const int g = th.g;
-    Cx<T>* xo = (g == 0 ? a.Xex : g == 1 ? a.Xey : a.Xev) + ro;
-    row_r2c_finish<RF>(base + g * ARR, th.lane, NTR, v, tb, [&](int k, Cx<T> X) {
-      st(xo + k, g == 2 ? X : ld(xo + k) + X);
-    }, sync);
+    Cx<T>* xo = (g == 0 ? a.Xex2 : g == 1 ? a.Xey2 : a.Xev) + ro;
+    row_r2c_finish<RF>(base + g * ARR, th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
   }
 }
 
 
 template <class T> struct ColFwdComArgs {
   Tables<T> tb;
-  const Cx<T>* X[11];
+  const Cx<T>* X[13];
   const Cx<T>* in[6];  // stage input (the state the RHS is evaluated at)
   T mu, eta;
   int forcing;
@@ -301,12 +301,14 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_c
   const T* ky = a.tb.ky;
   const int tid = threadIdx.x;
   Cx<T> v[P], d[P];
-  auto fft = [&](const Cx<T>* X) {
+  // forward transform of X (+ X2: two parts of one flux, summed as loaded)
+  auto fft = [&](const Cx<T>* X, const Cx<T>* X2 = nullptr) {
     __syncthreads();
     fft_run<F, -1>(sm, tid, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
       const int c = c0 + t;
       if (c >= Nh) return cx<T>(0, 0);
-      return ldg(X + (size_t)i * ld + c);
+      const size_t o = (size_t)i * ld + c;
+      return X2 ? ldg(X + o) + ldg(X2 + o) : ldg(X + o);
     }, SyncBlock{});
   };
   // visit the outputs of the last stage: g(idx, c, j, masked)
@@ -359,9 +361,9 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_c
       }
       break;
     case 3:  // -(i kx Ex + i ky Ey) + mu E_Visc_k                          (:412-413)
-      fft(a.X[XEX]);
+      fft(a.X[XEX], a.X[XEX2]);
       each([&](int q, int c, int j, bool m) { d[q] = m ? zero : ikmul(__ldg(kx + c), v[q]); });
-      fft(a.X[XEY]);
+      fft(a.X[XEY], a.X[XEY2]);
       each([&](int q, int c, int j, bool m) { d[q] = -(d[q] + (m ? zero : ikmul(__ldg(ky + j), v[q]))); });
       fft(a.X[XEV]);
       each([&](int q, int c, int j, bool m) { d[q] = d[q] + rmul(mu, m ? zero : v[q]); });
@@ -502,8 +504,8 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   r2.Hbx = w.H[HBX];
   r2.Hby = w.H[HBY];
   r2.Hikybx = w.H[HIKYBX];
-  r2.Xex = w.X[XEX];
-  r2.Xey = w.X[XEY];
+  r2.Xex2 = w.X[XEX2];
+  r2.Xey2 = w.X[XEY2];
   r2.Xev = w.X[XEV];
   r2.eta = p.eta;
   r2.inv_nx = (T)(1.0 / g.Nx);
@@ -512,7 +514,7 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
 
   ColFwdComArgs<T> cf{};
   cf.tb = g.tb;
-  for (int q = 0; q < 11; q++) cf.X[q] = w.X[q];
+  for (int q = 0; q < 13; q++) cf.X[q] = w.X[q];
   for (int q = 0; q < 6; q++) cf.in[q] = in[q];
   cf.mu = p.mu;
   cf.eta = p.eta;

@@ -35,11 +35,13 @@ template <class T> struct ComParamsT {
 };
 template <class T> struct ComWork {
   FieldPool<T> H;  // half-real: rho, rho_ux, rho_uy, E, Bx, By, d(uy)/dy, [iky Bx, ikx By]
-  FieldPool<T> X;  // x-transformed rows: ux, uy, Mxx, Mxy, Myy, Mag, Ex, Ey, EV, Fx, Fy
+  // x-transformed rows: ux, uy, Mxx, Mxy, Myy, Mag, Ex, Ey, EV, Fx, Fy, and the
+  // curl-B parts of Ex, Ey
+  FieldPool<T> X;
   int alloc(const Grid<T>& g, cudaStream_t st) {
     int s = H.alloc(g, 9, st);
     if (s) return s;
-    return X.alloc(g, 11, st);
+    return X.alloc(g, 13, st);
   }
   void release() { H.release(); X.release(); }
 };
