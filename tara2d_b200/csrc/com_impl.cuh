@@ -82,55 +82,59 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
     });
   }
   __syncthreads();
-  // phase 2: velocity                            (:105-106)
+  // flux q at one point                                                (:105-106, :193-213)
+  const T cs2 = a.cs2;
+  auto flux = [&](int qq, T rho, T mx, T my, T E, T bx, T by) -> T {
+    const T ux = mx / rho, uy = my / rho;
+    const T B2 = bx * bx + by * by;
+    const T Pr = cs2 * rho;
+    switch (qq) {
+      case XUX: return ux;
+      case XUY: return uy;
+      case XMXX: return mx * ux + Pr + B2 / (T)2 - bx * bx;
+      case XMXY: return mx * uy - bx * by;
+      case XMYY: return my * uy + Pr + B2 / (T)2 - by * by;
+      case XMAG: return uy * bx - by * ux;
+      case XEX: return (E + Pr + B2 / (T)2) * ux - ux * bx * bx - uy * bx * by;
+      default: return (E + Pr + B2 / (T)2) * uy - ux * bx * by - uy * by * by;  // XEY
+    }
+  };
+  // phase 2 (eight arrays): all eight fluxes of every point, once, in place
+  // (each point's six inputs are read before its eight outputs are written)
   if constexpr (!LOW) {
     for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
-      const Cx<T> rho = f[0][n], mx = f[1][n], my = f[2][n];
-      f[6][n] = cx<T>(mx.x / rho.x, mx.y / rho.y);
-      f[7][n] = cx<T>(my.x / rho.x, my.y / rho.y);
+      Cx<T> F[6];
+#pragma unroll
+      for (int k = 0; k < 6; k++) F[k] = f[k][n];
+      T o[8][2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const T rho = h ? F[0].y : F[0].x, mx = h ? F[1].y : F[1].x, my = h ? F[2].y : F[2].x;
+        const T E = h ? F[3].y : F[3].x, bx = h ? F[4].y : F[4].x, by = h ? F[5].y : F[5].x;
+#pragma unroll
+        for (int qq = 0; qq < 8; qq++) o[qq][h] = flux(qq, rho, mx, my, E, bx, by);
+      }
+#pragma unroll
+      for (int qq = 0; qq < 8; qq++) f[qq][n] = cx<T>(o[qq][0], o[qq][1]);
     }
     __syncthreads();
   }
-  // phase 3: fluxes of output th.g at the stage-0 points, then r2c     (:193-213)
-  const T cs2 = a.cs2;
+  // phase 3: flux th.g at the stage-0 points (six arrays: formed here), then r2c
   const int q = th.g;
   row_r2c_begin<RF>(th.lane, v, tb, [&](int n) -> Cx<T> {
-    Cx<T> F[8];
+    if constexpr (!LOW) {
+      return f[q][n];
+    } else {
+      Cx<T> F[6];
 #pragma unroll
-    for (int k = 0; k < NA; k++) F[k] = f[k][n];
-    T o[2];
+      for (int k = 0; k < 6; k++) F[k] = f[k][n];
+      T o[2];
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const T rho = h ? F[0].y : F[0].x;
-      const T mx = h ? F[1].y : F[1].x;
-      const T my = h ? F[2].y : F[2].x;
-      const T E = h ? F[3].y : F[3].x;
-      const T bx = h ? F[4].y : F[4].x;
-      const T by = h ? F[5].y : F[5].x;
-      T ux, uy;
-      if constexpr (LOW) {
-        ux = mx / rho;
-        uy = my / rho;
-      } else {
-        ux = h ? F[6].y : F[6].x;
-        uy = h ? F[7].y : F[7].x;
-      }
-      const T B2 = bx * bx + by * by;
-      const T Pr = cs2 * rho;
-      T r;
-      switch (q) {
-        case XUX: r = ux; break;
-        case XUY: r = uy; break;
-        case XMXX: r = mx * ux + Pr + B2 / (T)2 - bx * bx; break;
-        case XMXY: r = mx * uy - bx * by; break;
-        case XMYY: r = my * uy + Pr + B2 / (T)2 - by * by; break;
-        case XMAG: r = uy * bx - by * ux; break;
-        case XEX: r = (E + Pr + B2 / (T)2) * ux - ux * bx * bx - uy * bx * by; break;
-        default: r = (E + Pr + B2 / (T)2) * uy - ux * bx * by - uy * by * by; break;  // XEY
-      }
-      o[h] = r;
+      for (int h = 0; h < 2; h++)
+        o[h] = flux(q, h ? F[0].y : F[0].x, h ? F[1].y : F[1].x, h ? F[2].y : F[2].x, h ? F[3].y : F[3].x,
+                    h ? F[4].y : F[4].x, h ? F[5].y : F[5].x);
+      return cx<T>(o[0], o[1]);
     }
-    return cx<T>(o[0], o[1]);
   });
   __syncthreads();  // every group has its inputs: the field arrays are free
   Cx<T>* xo = a.X[q] + ro;
