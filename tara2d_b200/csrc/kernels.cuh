@@ -26,7 +26,7 @@ template <int L> struct ColFwdComCfg<double, L> {
   static constexpr int CB = (L <= 256) ? 8 : (L == 384 ? 4 : 2);
 };
 template <int L> struct ColFwdComCfg<float, L> {
-  static constexpr int P = (L == 384) ? 24 : (L >= 512 ? 8 : 16);
+  static constexpr int P = (L == 384) ? 24 : (L >= 512 && L < 4096 ? 8 : 16);
   static constexpr int CB = (L <= 256) ? 8 : (L >= 4096 ? 2 : 4);
 };
 // Row pass: P values per thread (M = Nx/2 points per row FFT).
