@@ -147,6 +147,7 @@ struct SessionT : tara_session {
 
   int apply_params() override {
     drop_graphs();
+    h_for = nullptr;
     if (p.Lx != g.Lx || p.Ly != g.Ly || p.pi != g.pi) {
       // wavenumber tables depend on Lx, Ly and pi
       TARA_CUDA_TRY(cudaStreamSynchronize(st));
@@ -218,6 +219,7 @@ struct SessionT : tara_session {
 
   int set_fields(int which, const double* const* h) override {
     if (!h) { set_error("null field array"); return TARA_EINVAL; }
+    if (which == 0) h_for = nullptr;
     for (int f = 0; f < nf; f++) TARA_TRY(h2d(h[f], pool(which)[f]));
     TARA_CUDA_TRY(cudaStreamSynchronize(st));
     return TARA_OK;
@@ -231,17 +233,30 @@ struct SessionT : tara_session {
   int rhs(Cx<T>* const* in, const StepArgs<T>& s) {
     switch (model) {
       case TARA_MODEL_COH: return coh_rhs(g, cw, cohp, in, s, st);
-      case TARA_MODEL_COM:
+      case TARA_MODEL_COM: {
         if constexpr (sizeof(T) == sizeof(double)) {
           if (clos) {  // the learned closure's stress/EMF spectra for this RHS input
             Cx<double>* out4[4] = {closf[0], closf[1], closf[2], closf[3]};
             TARA_TRY(closure_terms(clos, g, in, out4, st));
           }
         }
-        return com_rhs(g, mw, comp, in, s, st);
+        // the column-inverse pass runs only when mw.H does not already hold
+        // the y-inverse of this input; stepping RHS write it for the next input
+        comp.skip_inv = h_for == (const void*)in[0];
+        comp.fuse_inv = s.mode != STEP_RHS;
+        const int r = com_rhs(g, mw, comp, in, s, st);
+        if (s.mode == STEP_RHS) h_for = in[0];
+        else if (s.mode == STEP_RK4 && s.stage < 3) h_for = s.us[0];
+        else h_for = s.unew[0];
+        return r;
+      }
       default: return vort_rhs(g, vw, vortp, in, s, st);
     }
   }
+
+  // MHD: the field set whose y-inverse mw.H holds (nullptr: none)
+  const void* h_for = nullptr;
+  void invalidate_derived() override { h_for = nullptr; }
 
   // learned closure (MHD, FP64 sessions of the closure's coarse grid)
   tara_closure* clos = nullptr;
@@ -297,6 +312,7 @@ struct SessionT : tara_session {
   struct StepGraph {
     int stepper = -1;
     const void* ubase = nullptr;
+    bool hv = false;  // MHD: captured with mw.H holding the inverse of the state
     cudaGraphExec_t exec = nullptr;
   };
   StepGraph graphs[6];
@@ -308,19 +324,22 @@ struct SessionT : tara_session {
   }
   cudaGraphExec_t pair_graph(int stepper) {
     for (auto& gr : graphs)
-      if (gr.exec && gr.stepper == stepper && gr.ubase == u.base) return gr.exec;
+      if (gr.exec && gr.stepper == stepper && gr.ubase == u.base && gr.hv == (h_for == (const void*)u[0]))
+        return gr.exec;
     StepGraph* slot = nullptr;
     for (auto& gr : graphs)
       if (!gr.exec) { slot = &gr; break; }
     if (!slot) { drop_graphs(); slot = &graphs[0]; }
     const void* ub = u.base;
     const FieldPool<T> u0 = u, unew0 = unew;
+    const void* h0 = h_for;
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return nullptr;
     int r = launch_steps(stepper, 2);
     cudaError_t e = cudaStreamEndCapture(st, &graph);
     u = u0;  // nothing ran while capturing
     unew = unew0;
+    h_for = h0;
     cudaGetLastError();
     cudaGraphExec_t exec = nullptr;
     if (r == TARA_OK && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) exec = nullptr;
@@ -329,6 +348,7 @@ struct SessionT : tara_session {
     if (!exec) return nullptr;
     slot->stepper = stepper;
     slot->ubase = ub;
+    slot->hv = h0 == (const void*)u[0];
     slot->exec = exec;
     return exec;
   }
@@ -344,10 +364,17 @@ struct SessionT : tara_session {
       return TARA_EINVAL;
     }
     int done = 0;
-    if (use_graphs && !prof.on && n >= 2) {
+    if (model == TARA_MODEL_COM && n >= 1 && h_for != (const void*)u[0]) {
+      // one step with the column-inverse pass; after it mw.H holds the inverse
+      // of the state, as the graphs (captured in that condition) assume
+      TARA_TRY(launch_steps(stepper, 1));
+      done = 1;
+    }
+    if (use_graphs && !prof.on && n - done >= 2) {
       cudaGraphExec_t ex = pair_graph(stepper);
       if (ex) {
         // capture swapped u/unew twice: the state is back in the same buffer
+        // (and mw.H, for MHD, again holds its inverse)
         for (; done + 2 <= n; done += 2) TARA_CUDA_TRY(cudaGraphLaunch(ex, st));
       }
     }
@@ -392,6 +419,7 @@ struct SessionT : tara_session {
   int elementwise(int mode, int nfld, const double* const* u, const double* const* d1,
                   const double* const* d2, double* const* out) override {
     if (!u || !d1 || !d2 || !out) { set_error("null field array"); return TARA_EINVAL; }
+    h_for = nullptr;
     Cx<T>* du[6];
     Cx<T>* dd1[6];
     Cx<T>* dd2[6];
@@ -459,6 +487,7 @@ struct SessionT : tara_session {
   int real_fields(int what, double* const* h) override {
     if (!h) { set_error("null field array"); return TARA_EINVAL; }
     TARA_TRY(ensure_real());
+    h_for = nullptr;  // the transforms use the work pool
     const size_t nn = (size_t)Nx * Ny;
     T* r[9];
     for (int q = 0; q < nf + 3; q++) r[q] = rbuf + q * nn;
@@ -496,6 +525,7 @@ struct SessionT : tara_session {
   int set_state_real(const double* const* h) override {
     if (!h) { set_error("null field array"); return TARA_EINVAL; }
     TARA_TRY(ensure_real());
+    h_for = nullptr;
     const size_t nn = (size_t)Nx * Ny;
     const T* r[6];
     Cx<T>* st_[6];
@@ -520,6 +550,7 @@ struct SessionT : tara_session {
 
   int num_shells() override { return diag_num_shells(Nx, Ny, p.Lx, p.Ly, p.pi); }
   int record(double* drec) {
+    h_for = nullptr;  // the diagnostics use the work pool
     if (!dw.mem || dw.nbins != num_shells()) {
       dw.release();
       TARA_TRY(dw.alloc(g, st));

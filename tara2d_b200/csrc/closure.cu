@@ -479,6 +479,7 @@ int tara_filter_state(tara_session* fine, tara_session* coarse) {
                                           static_cast<Cx<double>*>(coarse->state_ptr(k)), coarse->Nx, cg.ld, scale);
   TARA_CUDA_TRY(cudaGetLastError());
   TARA_CUDA_TRY(cudaStreamSynchronize(coarse->st));
+  coarse->invalidate_derived();
   return TARA_OK;
 }
 

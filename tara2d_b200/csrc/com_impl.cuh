@@ -289,6 +289,11 @@ template <class T> struct ColFwdComArgs {
   int forcing;
   int closure;            // add the subgrid stress / EMF spectra of clos[]
   const Cx<T>* clos[4];   // tau_xx, tau_xy, tau_yy, EMF
+  // fuse: also y-invert the next RHS input of field f into hnext[f] (and
+  // i ky Bx into hikybx when set), the next RHS's column-inverse pass
+  int fuse;
+  Cx<T>* hnext[6];
+  Cx<T>* hikybx;
   StepArgs<T> step;
 };
 
@@ -396,7 +401,30 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_c
     const int c = c0 + t;
     idx = (size_t)i * ld + c;
     return c < Nh;
-  }, d);
+  }, d, a.fuse ? d : nullptr);
+  if (!a.fuse) return;
+  // y-inverse of the next RHS input of these columns (it is in d, at the
+  // forward transform's output positions): through the exchange tile, then
+  // an inverse transform, stored as the next column-inverse pass would
+  auto invert = [&](Cx<T>* dst, int mul) {
+    __syncthreads();  // the exchange tile is free
+#pragma unroll
+    for (int e = 0; e < P; e++) {
+      int t, i;
+      F::template out_pos<F::S - 1>(tid, e / RL, e % RL, t, i);
+      sm[F::sidx(t, i)] = d[e];
+    }
+    __syncthreads();
+    fft_run<F, +1>(sm, tid, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) {
+      return apply_ymul(mul, __ldg(ky + i), sm[F::sidx(t, i)]);
+    }, SyncBlock{});
+    fft_emit<F>(tid, v, [&](int t, int i, Cx<T> x) {
+      const int c = c0 + t;
+      if (c < Nh) st(dst + (size_t)i * ld + c, x);
+    });
+  };
+  invert(a.hnext[f], MUL_ONE);
+  if (f == 4 && a.hikybx) invert(a.hikybx, MUL_IKY);
 }
 
 template <int L, class T>
@@ -464,13 +492,15 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
     return TARA_EUNSUPPORTED;
   }
   const int forcing = p.A != (T)0;
-  ColInvArgs<T> ci{};
-  ci.tb = g.tb;
-  for (int q = 0; q < 6; q++) ci.job[q] = ColInvJob<T>{in[q], w.H[q], MUL_ONE};
-  int nj = 6;
-  if (p.fix_curlB) ci.job[nj++] = ColInvJob<T>{in[4], w.H[HIKYBX], MUL_IKY};
-  prof_mark(g.prof, st, KK_COL_INV);
-  run_col_inv(ci, nj, st);
+  if (!p.skip_inv) {  // else w.H already holds the y-inverse of `in` (previous column pass)
+    ColInvArgs<T> ci{};
+    ci.tb = g.tb;
+    for (int q = 0; q < 6; q++) ci.job[q] = ColInvJob<T>{in[q], w.H[q], MUL_ONE};
+    int nj = 6;
+    if (p.fix_curlB) ci.job[nj++] = ColInvJob<T>{in[4], w.H[HIKYBX], MUL_IKY};
+    prof_mark(g.prof, st, KK_COL_INV);
+    run_col_inv(ci, nj, st);
+  }
 
   RowCom1Args<T> r1{};
   r1.tb = g.tb;
@@ -525,6 +555,9 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   cf.forcing = forcing;
   cf.closure = p.closure;
   for (int q = 0; q < 4; q++) cf.clos[q] = p.clos[q];
+  cf.fuse = p.fuse_inv && step.mode != STEP_RHS;
+  for (int q = 0; q < 6; q++) cf.hnext[q] = w.H[q];
+  cf.hikybx = p.fix_curlB ? w.H[HIKYBX] : nullptr;
   cf.step = step;
   prof_mark(g.prof, st, KK_COL_FWD_COM);
   TARA_DISPATCH_LEN(g.Ny, col_fwd_com_dispatch, cf, st)

@@ -284,8 +284,11 @@ __device__ __forceinline__ void step_apply(const StepArgs<T>& s, int f, size_t i
 // they never alias), so a thread would wait on memory N times in a row.
 // pos(e, idx) gives element e's index and whether it exists.  Same
 // arithmetic as step_apply, element for element.
+// nxt (optional, may be d): receives each element's next RHS input (the new
+// state, or the next RK4 stage input).
 template <class T, int N, class POS>
-__device__ __forceinline__ void step_apply_n(const StepArgs<T>& s, int f, POS&& pos, const Cx<T>* d) {
+__device__ __forceinline__ void step_apply_n(const StepArgs<T>& s, int f, POS&& pos, const Cx<T>* d,
+                                             Cx<T>* nxt = nullptr) {
   if (s.mode == STEP_RHS) {
 #pragma unroll
     for (int e = 0; e < N; e++) {
@@ -312,24 +315,39 @@ __device__ __forceinline__ void step_apply_n(const StepArgs<T>& s, int f, POS&& 
 #pragma unroll
   for (int e = 0; e < N; e++) {
     size_t idx;
-    if (!pos(e, idx)) continue;
+    const bool ok = pos(e, idx);
     const Cx<T> de = d[e];
+    Cx<T> nv = cx<T>(0, 0);
     if (s.mode == STEP_AB2) {
       const Cx<T> inc = rmul((T)1.5, de) - rmul((T)0.5, x0[e]);
-      st(s.unew[f] + idx, x1[e] + rmul(s.dt, inc));
-      st(s.dold[f] + idx, de);
+      nv = x1[e] + rmul(s.dt, inc);
+      if (ok) {
+        st(s.unew[f] + idx, nv);
+        st(s.dold[f] + idx, de);
+      }
     } else if (s.mode == STEP_EULER) {
-      st(s.unew[f] + idx, x1[e] + rmul(s.dt, de));
-      st(s.dold[f] + idx, de);
+      nv = x1[e] + rmul(s.dt, de);
+      if (ok) {
+        st(s.unew[f] + idx, nv);
+        st(s.dold[f] + idx, de);
+      }
     } else if (s.stage == 0) {
-      st(s.acc[f] + idx, x1[e] + rmul(s.wa, de));
-      st(s.us[f] + idx, x1[e] + rmul(s.cs, de));
+      nv = x1[e] + rmul(s.cs, de);
+      if (ok) {
+        st(s.acc[f] + idx, x1[e] + rmul(s.wa, de));
+        st(s.us[f] + idx, nv);
+      }
     } else if (s.stage < 3) {
-      st(s.acc[f] + idx, x0[e] + rmul(s.wa, de));
-      st(s.us[f] + idx, x1[e] + rmul(s.cs, de));
+      nv = x1[e] + rmul(s.cs, de);
+      if (ok) {
+        st(s.acc[f] + idx, x0[e] + rmul(s.wa, de));
+        st(s.us[f] + idx, nv);
+      }
     } else {
-      st(s.unew[f] + idx, x0[e] + rmul(s.wa, de));
+      nv = x0[e] + rmul(s.wa, de);
+      if (ok) st(s.unew[f] + idx, nv);
     }
+    if (nxt) nxt[e] = ok ? nv : cx<T>(0, 0);
   }
 }
 

@@ -27,11 +27,15 @@ constexpr int kCohLaunches = 3;
 // ---- compressible MHD, src/derive2com.f95 ----
 // closure != 0: the spectra of a subgrid stress (xx, xy, yy) and EMF in
 // clos[] are added to the momentum and induction fluxes (learned closure).
+// skip_inv: the half-real fields H already hold the y-inverse of the RHS
+// input (written by the previous column-forward pass); fuse_inv: the
+// column-forward pass writes H for the next RHS input (stepping modes).
 template <class T> struct ComParamsT {
   T mu, eta, cs2, kf, A;
   int fix_curlB;
   int closure;
   const Cx<T>* clos[4];
+  int skip_inv, fuse_inv;
 };
 template <class T> struct ComWork {
   FieldPool<T> H;  // half-real: rho, rho_ux, rho_uy, E, Bx, By, d(uy)/dy, [iky Bx, ikx By]
@@ -48,7 +52,9 @@ template <class T> struct ComWork {
 template <class T>
 int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* const in[6],
             const StepArgs<T>& step, cudaStream_t st);
-constexpr int kComLaunches = 5;
+// per RHS evaluation while stepping: the column-inverse pass of the next RHS
+// is fused into the column-forward pass (one more launch where a run starts)
+constexpr int kComLaunches = 4;
 
 // ---- incompressible (screened) vorticity, src/derive2csh.f95, src/derive2css.f95 ----
 template <class T> struct VortParamsT { T nu, alpha, lambda; int screened; };

@@ -53,4 +53,7 @@ struct tara_session {
   virtual const void* grid_ptr() const = 0;
   virtual void* state_ptr(int q) = 0;
   virtual int attach_closure(tara_closure* c) = 0;
+  // the state was changed from outside the stepping kernels: drop what was
+  // derived from it
+  virtual void invalidate_derived() = 0;
 };
