@@ -120,18 +120,21 @@ def field_bytes(esize=16):
 
 def kernel_bytes_per_launch(name: str) -> float:
     """Algorithmic bytes of one launch: every field a kernel must read or
-    write, once (S = one spectral field, Ny*(Nx/2+1)*16 B in FP64).  The
-    RK4 epilogue of k_col_fwd_com is averaged over its four stages
-    (stage 0: u read, acc and next-stage written = 18 S; stages 1-2: stage
-    input (4 fields) + u + acc read, acc and next-stage written = 28 S;
-    stage 3: stage input (4) + acc read, new state written = 16 S)."""
+    write, once (S = one spectral field, Ny*(Nx/2+1)*16 B in FP64).
+    k_col_fwd_com reads the 11 x-transformed fluxes and writes the y-inverse
+    of the next RHS input (6 fields); its RK4 epilogue is averaged over the
+    four stages (stage 0: u read, acc and next-stage written = 18 S; stages
+    1-2: stage input (4 fields) + u + acc read, acc and next-stage written =
+    28 S; stage 3: stage input (4) + acc read, new state written = 16 S).
+    k_col_inv runs only where a run starts (the column-forward pass does the
+    next RHS's y-inverse while stepping)."""
     S = field_bytes()
     table = {
         "k_col_inv": 12 * S,        # 6 state fields in, 6 half-real out
         "k_row_com1": 14 * S,       # 6 in, 8 out (ux, uy, Mxx, Mxy, Myy, Mag, Ax, Ay)
         "k_col_rt": 2 * S,          # X(uy) in, d(uy)/dy out
-        "k_row_com2": 9 * S,        # X(ux), H(duy), H(Bx), H(By), X(Ex), X(Ey) in; X(Ex), X(Ey), X(EV) out
-        "k_col_fwd_com": 9 * S + (18 + 28 + 28 + 16) / 4.0 * S,
+        "k_row_com2": 7 * S,        # X(ux), H(duy), H(Bx), H(By) in; the curl-B energy-flux parts and EV out
+        "k_col_fwd_com": 11 * S + (18 + 28 + 28 + 16) / 4.0 * S + 6 * S,
     }
     return table.get(name, 0.0)
 
