@@ -136,6 +136,20 @@ int tara_set_state_real(tara_session* s, const double* const* fields);
 int tara_write_snapshot(tara_session* s, const char* path);
 int tara_format_list_directed(const double* v, int n, char* out, int cap);
 
+/* ---- binary checkpoint / restart (no counterpart in the reference, whose
+ * drivers always start from an initial condition: src/main2com.f95:215-343,
+ * src/main2coh.f95:176-257) ----
+ * tara_checkpoint_write: state, AB2/Euler history, model, grid, parameters
+ * and the caller's step count and time to one binary file (FP64 whatever the
+ * precision; written to path.tmp, then renamed over path).
+ * tara_checkpoint_read: restores parameters, state and history into a session
+ * of the same model and grid (the precision may differ) and returns the
+ * stored step and time (either pointer may be NULL).  TARA_EINVAL with
+ * tara_last_error() set for a missing, truncated or corrupted file (checksum)
+ * or a model/grid mismatch.  Layout: tara2d_b200/csrc/checkpoint.cu. */
+int tara_checkpoint_write(tara_session* s, const char* path, long long step, double time);
+int tara_checkpoint_read(tara_session* s, const char* path, long long* step, double* time);
+
 /* ---- learned subgrid closure of the MHD path (no counterpart in the
  * reference) ----
  * A CNN of four periodic 3x3 convolutions (5 -> 32 -> 32 -> 32 -> 4 channels,

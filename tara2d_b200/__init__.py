@@ -111,6 +111,8 @@ def lib():
         L.tara_set_state_real.argtypes = [P, PP]
         L.tara_get_vorticity_real.argtypes = [P, P]
         L.tara_write_snapshot.argtypes = [P, C.c_char_p]
+        L.tara_checkpoint_write.argtypes = [P, C.c_char_p, C.c_longlong, D]
+        L.tara_checkpoint_read.argtypes = [P, C.c_char_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
         L.tara_format_list_directed.argtypes = [P, I, C.c_char_p, I]
         L.tara_ens_open.argtypes = [C.POINTER(C.c_void_p), I, I, P, C.POINTER(Params), I]
         L.tara_ens_close.argtypes = [P]
@@ -251,6 +253,25 @@ class Session:
     def write_snapshot(self, path: str) -> None:
         """The drivers' grid file (fort.NNNNNNNN) of the current state."""
         check(lib().tara_write_snapshot(self._h, os.fsencode(path)), "tara_write_snapshot")
+
+    def checkpoint(self, path: str, step: int = 0, time: float = 0.0) -> None:
+        """Binary checkpoint of state, history, parameters, step and time
+        (format: tara2d_b200.checkpoint)."""
+        check(lib().tara_checkpoint_write(self._h, os.fsencode(path), int(step), float(time)),
+              "tara_checkpoint_write")
+
+    def restore(self, path: str):
+        """Restore parameters, state and history from a checkpoint of the same
+        model and grid; returns its (step, time)."""
+        step, time = C.c_longlong(), C.c_double()
+        check(lib().tara_checkpoint_read(self._h, os.fsencode(path), C.byref(step), C.byref(time)),
+              "tara_checkpoint_read")
+        from .checkpoint import read_header
+        h = read_header(path)
+        for k, v in h["params"].items():
+            setattr(self.params, "lambda_" if k == "lambda" else k, v)
+        self.params.fix_curlB = h["fix_curlB"]
+        return step.value, time.value
 
     def set_graphs(self, on: bool) -> None:
         """Replay steps from CUDA graphs (default) or launch every kernel from the host."""

@@ -14,7 +14,9 @@
 //                  to the energy fluxes                      (:183-209)
 //   k_col_fwd_com  y-forward, i k multiplies, k^2 terms, dealiasing and the
 //                  assembly of the six derivatives          (:262-419), fused with
-//                  the stepper update.
+//                  the stepper update and, while stepping, with the y-inverse
+//                  of the next RHS input (k_col_inv then runs only where a
+//                  run starts).
 //
 // Mom_y_1 is Mom_x_2 (src/derive2com.f95:197, :199) and Mag_y is -Mag_x
 // exactly (:212-213), so each is transformed once.  The reference also
