@@ -136,6 +136,33 @@ int tara_set_state_real(tara_session* s, const double* const* fields);
 int tara_write_snapshot(tara_session* s, const char* path);
 int tara_format_list_directed(const double* v, int n, char* out, int cap);
 
+/* ---- seeded initial conditions built on the device ----
+ * The benchmark configurations' ICs, replacing the drivers' host-side IC
+ * construction and r2c (src/main2coh.f95:141-222, src/main2com.f95:230-300).
+ * A solenoidal random-phase field has psi_k = a(|k|) e^{2 pi i U} on every
+ * half-spectrum mode, a = sqrt(E(|k|)/|k|^3), U a counter-based uniform of
+ * (seed, stream, mode) (layout and generator: tara2d_b200/csrc/ic.cu; the
+ * host restatement tara2d_b200.initial.hashed_state gives the same state).
+ *   TARA_IC_RANDOM_PHASE, hydro: u with E(k) ~ k^4 exp(-(k/k0)^2) and
+ *     <|u|^2>/2 = e1; density 1 + e2 N(0,1).
+ *   TARA_IC_RANDOM_PHASE, MHD: rho = 1, u and B as above with energies e1, e2.
+ *   TARA_IC_ORSZAG_TANG, MHD: u = (-sin y, sin x), B = (-sin y, sin 2x), rho = 1,
+ *     plus random-phase perturbations with E(k) ~ k on kmin <= |k| <= kmax of
+ *     rms e1 (u) and e2 (B).
+ * MHD: P = CS^2 rho, E = P/(spheat-1) + rho|u|^2/2 + |B|^2/2.  The state is
+ * replaced; the AB2 history is left as it is.  Vorticity models:
+ * TARA_EUNSUPPORTED. */
+#define TARA_IC_RANDOM_PHASE 1
+#define TARA_IC_ORSZAG_TANG 2
+typedef struct {
+  int kind;
+  int reserved0;
+  unsigned long long seed;
+  double k0, e1, e2, kmin, kmax;
+  double reserved[3];
+} tara_ic;
+int tara_set_state_random(tara_session* s, const tara_ic* ic);
+
 /* ---- binary checkpoint / restart (no counterpart in the reference, whose
  * drivers always start from an initial condition: src/main2com.f95:215-343,
  * src/main2coh.f95:176-257) ----

@@ -39,6 +39,16 @@ class TaraError(RuntimeError):
     pass
 
 
+class IcDesc(C.Structure):
+    """tara_ic (include/tara2d_gpu.h): a seeded initial condition built on the device."""
+    _fields_ = [("kind", C.c_int), ("reserved0", C.c_int), ("seed", C.c_ulonglong), ("k0", C.c_double),
+                ("e1", C.c_double), ("e2", C.c_double), ("kmin", C.c_double), ("kmax", C.c_double),
+                ("reserved", C.c_double * 3)]
+
+
+IC_RANDOM_PHASE, IC_ORSZAG_TANG = 1, 2
+
+
 class Params(C.Structure):
     """tara_params (include/tara2d_gpu.h)."""
     _fields_ = [(n, C.c_double) for n in
@@ -112,6 +122,7 @@ def lib():
         L.tara_get_vorticity_real.argtypes = [P, P]
         L.tara_write_snapshot.argtypes = [P, C.c_char_p]
         L.tara_checkpoint_write.argtypes = [P, C.c_char_p, C.c_longlong, D]
+        L.tara_set_state_random.argtypes = [P, C.POINTER(IcDesc)]
         L.tara_checkpoint_read.argtypes = [P, C.c_char_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
         L.tara_format_list_directed.argtypes = [P, I, C.c_char_p, I]
         L.tara_ens_open.argtypes = [C.POINTER(C.c_void_p), I, I, P, C.POINTER(Params), I]
@@ -253,6 +264,16 @@ class Session:
     def write_snapshot(self, path: str) -> None:
         """The drivers' grid file (fort.NNNNNNNN) of the current state."""
         check(lib().tara_write_snapshot(self._h, os.fsencode(path)), "tara_write_snapshot")
+
+    def set_state_random(self, kind: int, seed: int, k0: float = 4.0, e1: float = 0.5, e2: float = 0.01,
+                         kmin: float = 0.0, kmax: float = 0.0) -> None:
+        """State from a seeded initial condition built on the device
+        (IC_RANDOM_PHASE: hydro u energy e1 and density noise e2, or MHD
+        kinetic / magnetic energies e1, e2; IC_ORSZAG_TANG (MHD): perturbation
+        rms e1 (u), e2 (B) on kmin <= |k| <= kmax).  The host restatement
+        initial.hashed_state builds the same state."""
+        d = IcDesc(kind=kind, seed=seed, k0=k0, e1=e1, e2=e2, kmin=kmin, kmax=kmax)
+        check(lib().tara_set_state_random(self._h, C.byref(d)), "tara_set_state_random")
 
     def checkpoint(self, path: str, step: int = 0, time: float = 0.0) -> None:
         """Binary checkpoint of state, history, parameters, step and time

@@ -11,6 +11,7 @@
 #include "closure.h"
 #include "diag.cuh"
 #include "output.h"
+#include "ic.cuh"
 #include "realspace.cuh"
 #include "session.h"
 
@@ -548,6 +549,28 @@ struct SessionT : tara_session {
     return device_status();
   }
 
+  int set_state_random(const tara_ic* ic) override {
+    if (!ic) { set_error("null initial-condition description"); return TARA_EINVAL; }
+    TARA_TRY(ensure_real());
+    h_for = nullptr;
+    const size_t nn = (size_t)Nx * Ny;
+    T* r[9];
+    for (int q = 0; q < nf + 3; q++) r[q] = rbuf + q * nn;
+    if (workpool().count < nf || workpool().count < 4) { set_error("work pool too small"); return TARA_EINVAL; }
+    Cx<T>* wk[6];
+    for (int q = 0; q < 6; q++) wk[q] = q < workpool().count ? workpool()[q] : nullptr;
+    TARA_TRY(ic_random_state<T>(g, model, p, *ic, r, wk, st));
+    const T* rc[6];
+    Cx<T>* st_[6];
+    for (int q = 0; q < nf; q++) {
+      rc[q] = r[q];
+      st_[q] = u[q];
+    }
+    TARA_TRY(real_to_state(g, nf, rc, st_, wk, st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return device_status();
+  }
+
   int num_shells() override { return diag_num_shells(Nx, Ny, p.Lx, p.Ly, p.pi); }
   int record(double* drec) {
     h_for = nullptr;  // the diagnostics use the work pool
@@ -769,6 +792,9 @@ int tara_get_vorticity_real(tara_session* s, double* omega) {
 }
 int tara_set_state_real(tara_session* s, const double* const* fields) {
   return s ? s->fail_if(s->set_state_real(fields)) : TARA_EINVAL;
+}
+int tara_set_state_random(tara_session* s, const tara_ic* ic) {
+  return s ? s->fail_if(s->set_state_random(ic)) : TARA_EINVAL;
 }
 
 // The drivers' grid files: one line per grid point, x outer, y inner, as

@@ -159,9 +159,9 @@ __global__ void __launch_bounds__(CB * L / P, 1) k_col_inv_tma(const __grid_cons
   using F = FFTB<L, CB, P>;
   using LY = ColTmaLayout<L, CB, P>;
   constexpr unsigned TILE_BYTES = (unsigned)(CB * L * sizeof(Cx<T>));
-  extern __shared__ __align__(128) unsigned char smraw[];
-  Cx<T>* buf0 = reinterpret_cast<Cx<T>*>(smraw);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + 2 * (size_t)LY::BUFE * sizeof(Cx<T>));
+  extern __shared__ __align__(128) unsigned char smtile[];  // TMA destinations: 128-byte aligned
+  Cx<T>* buf0 = reinterpret_cast<Cx<T>*>(smtile);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smtile + 2 * (size_t)LY::BUFE * sizeof(Cx<T>));
   const int tid = threadIdx.x;
   const int nitems = a.ntiles * a.njobs;
   const int Nh = a.tb.Nh, ld = a.tb.ld;

@@ -44,6 +44,8 @@ struct tara_session {
   // what = 0: the nf state fields in real space (c2r / NxNy); 1: vorticity
   virtual int real_fields(int what, double* const* h) = 0;
   virtual int set_state_real(const double* const* h) = 0;
+  // the state from a seeded initial condition built on the device
+  virtual int set_state_random(const tara_ic* ic) = 0;
   // nrec diagnostics records of the state, one before the first step and one
   // after every `every` steps (nsteps = (nrec - 1) * every), into rec
   // (host, nrec * (TARA_DIAG_VALUES + num_shells()) doubles)

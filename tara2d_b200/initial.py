@@ -127,3 +127,87 @@ def vorticity_random_phase(Nx, Ny, seed=0, k0=4.0, energy=0.5):
     KX, KY = _kgrid_full(Nx, Ny)
     w = np.real(np.fft.ifft2(1j * KX * np.fft.fft2(uy) - 1j * KY * np.fft.fft2(ux)))
     return [r2c(w)]
+
+
+# ---------------------------------------------------------------------------
+# Counter-based seeded initial conditions: the host restatement of the
+# device generator (tara_set_state_random, csrc/ic.cu).  Every random value
+# is a function of (seed, stream, index) only, so host and device build the
+# same state; FFTs and math functions differ only in rounding.
+IC_RANDOM_PHASE, IC_ORSZAG_TANG = 1, 2
+_M1, _M2 = np.uint64(0xBF58476D1CE4E5B9), np.uint64(0x94D049BB133111EB)
+_C1, _C2 = np.uint64(0xD1B54A32D192ED03), np.uint64(0x9E3779B97F4A7C15)
+
+
+def splitmix64_mix(z):
+    """The splitmix64 finaliser (S. Vigna): xor-shift 30, multiply, xor-shift 27,
+    multiply, xor-shift 31, modulo 2**64 (uint64 arrays)."""
+    z = np.asarray(z, dtype=np.uint64)
+    z = (z ^ (z >> np.uint64(30))) * _M1
+    z = (z ^ (z >> np.uint64(27))) * _M2
+    return z ^ (z >> np.uint64(31))
+
+
+def hashed_uniform(seed: int, stream: int, index) -> np.ndarray:
+    """u in [0, 1): mix(mix(seed ^ stream*C1) + (index+1)*C2) >> 11, times 2**-53."""
+    key = splitmix64_mix(np.array([seed], dtype=np.uint64) ^ (np.array([stream], dtype=np.uint64) * _C1))
+    idx = np.asarray(index, dtype=np.uint64)
+    v = splitmix64_mix(key + (idx + np.uint64(1)) * _C2)
+    return (v >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+
+
+def _half_k(Nx, Ny, Lx, Ly, pi):
+    Nh = Nx // 2 + 1
+    kx = 2.0 * pi * np.arange(Nh, dtype=np.float64) / Lx
+    j = np.arange(Ny, dtype=np.float64)
+    ky = np.where(np.arange(Ny) < Ny // 2, 2.0 * pi * j / Ly, 2.0 * pi * (j - Ny) / Ly)
+    return np.meshgrid(kx, ky)  # (Ny, Nh)
+
+
+def hashed_solenoidal(Nx, Ny, seed, stream, peaked, k0, kmin=0.0, kmax=np.inf, Lx=2 * PI, Ly=2 * PI, pi=PI):
+    """(u, v, mean(u^2 + v^2)) of the random-phase streamfunction of stream
+    `stream`: psi_k = a e^{2 pi i U(seed, stream, j*Nh + i)} on the half spectrum,
+    a = sqrt(E(k)/k^3), E = k^4 exp(-(k/k0)^2) (peaked) or k."""
+    KX, KY = _half_k(Nx, Ny, Lx, Ly, pi)
+    Nh = Nx // 2 + 1
+    K = np.sqrt(KX * KX + KY * KY)
+    amp = np.zeros_like(K)
+    sel = (K > 0) & (K >= kmin) & (K <= kmax)
+    k = K[sel]
+    e = k * k * k * k * np.exp(-(k / k0) * (k / k0)) if peaked else k
+    amp[sel] = np.sqrt(e / (k * k * k))
+    th = 2.0 * PI * hashed_uniform(seed, stream, np.arange(Ny * Nh)).reshape(Ny, Nh)
+    px, py = amp * np.cos(th), amp * np.sin(th)
+    u = np.fft.irfft2((-KY * py) + 1j * (KY * px), s=(Ny, Nx))
+    v = np.fft.irfft2((KX * py) + 1j * (-KX * px), s=(Ny, Nx))
+    return u, v, float(np.sum(u * u + v * v)) / (Nx * Ny)
+
+
+def hashed_state(model, Nx, Ny, kind, seed, k0=4.0, e1=0.5, e2=0.01, kmin=0.0, kmax=np.inf, Lx=2 * PI,
+                 Ly=2 * PI, pi=PI, CS=100.0, spheat=5.0 / 3.0):
+    """Spectral state of the device initial condition `kind` (model 1: hydro,
+    2: MHD), the same as tara_set_state_random builds (see include/tara2d_gpu.h)."""
+    ot = kind == IC_ORSZAG_TANG
+    lo, hi = (kmin, kmax) if ot else (0.0, np.inf)
+
+    def scale(msq, e):
+        if not msq > 0:
+            return 0.0
+        return e / np.sqrt(msq) if ot else np.sqrt(e / (0.5 * msq))
+
+    u, v, msq = hashed_solenoidal(Nx, Ny, seed, 1, not ot, k0, lo, hi, Lx, Ly, pi)
+    su = scale(msq, e1)
+    if model == 1:
+        n = Nx * Ny
+        k = np.arange(n, dtype=np.uint64)
+        u1 = 1.0 - hashed_uniform(seed, 3, 2 * k)
+        u2 = hashed_uniform(seed, 3, 2 * k + np.uint64(1))
+        g = (np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * PI * u2)).reshape(Ny, Nx)
+        return [r2c(1.0 + e2 * g), r2c(su * u), r2c(su * v)]
+    bu, bv, msq = hashed_solenoidal(Nx, Ny, seed, 2, not ot, k0, lo, hi, Lx, Ly, pi)
+    sb = scale(msq, e2)
+    ux, uy, bx, by = su * u, su * v, sb * bu, sb * bv
+    if ot:
+        X, Y = grid(Nx, Ny, Lx, Ly)
+        ux, uy, bx, by = ux - np.sin(Y), uy + np.sin(X), bx - np.sin(Y), by + np.sin(2.0 * X)
+    return com_state(np.ones((Ny, Nx)), ux, uy, bx, by, CS, spheat)
