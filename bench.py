@@ -71,7 +71,7 @@ class ClockSampler:
     def __init__(self, bus_id):
         self.bus_id = bus_id
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(ROOT, "bench_clocks", f"clocks_{os.getpid()}.csv")
 
     def start(self):
         try:

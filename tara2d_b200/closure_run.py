@@ -1,5 +1,5 @@
 """The learned-closure workload: data from a fine DNS, training, and the
-coarse closed run judged against a held-out DNS.
+coarse closed run compared with a held-out DNS.
 
     python -m tara2d_b200.closure_run train    --out DIR [options]
     python -m tara2d_b200.closure_run evaluate --out DIR [options]
