@@ -255,6 +255,53 @@ def run_ensemble(args):
     return 0
 
 
+# ------------------------------------------------------------------ ranks
+class Ranks:
+    """One process per GPU (replicas: the path does not shard).  Rank and
+    world size come from the launcher's environment (RANK, WORLD_SIZE,
+    LOCAL_RANK, MASTER_ADDR/PORT); the barrier and the max-over-ranks
+    reduction of the device time are the only collectives.  backend: "nccl"
+    on GPUs, "gloo" for the CPU tests of this logic."""
+
+    def __init__(self, backend: str = "nccl"):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        self.device = "cpu"
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.device = f"cuda:{self.local}"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def job_value(self, steps: int, ms_max: float) -> float:
+        """Whole-job steps/s: every rank ran `steps` steps; time = the slowest rank's."""
+        return self.world * steps / (ms_max / 1e3)
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     ap = argparse.ArgumentParser()
@@ -276,16 +323,8 @@ def main():
     if args.workload == "ensemble":
         return run_ensemble(args)
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ranks = Ranks("nccl")
+    world, rank, local = ranks.world, ranks.rank, ranks.local
 
     import tara2d_b200 as T
     T.set_device(local if world > 1 else 0)
@@ -297,17 +336,7 @@ def main():
     sess.step(T.STEP_RK4, W)
     sess.synchronize()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     try:
         bus = T.device_pci_bus_id()
@@ -321,7 +350,7 @@ def main():
     barrier()
     ms = max_over_ranks(ms)
     per_gpu = K / (ms / 1e3)
-    value = world * per_gpu
+    value = ranks.job_value(K, ms)
     launches = sess.launches_per_step(T.STEP_RK4) * K
 
     # per-kernel device times (events around every launch), same workload
@@ -388,9 +417,7 @@ def main():
                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
                "gpu_launches": launches}
         print(json.dumps(out), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
