@@ -114,7 +114,12 @@ __device__ __forceinline__ void row_coh_rows(const RowCohArgs<T>& a, int y0, Cx<
 }
 
 template <class T, int M, int P>
-__global__ void __launch_bounds__(TARA_ROW_LB(11 * (M / P))) k_row_coh(const RowCohArgs<T> a) {
+// Two CTAs per SM where a row's CTA has at most 352 threads (their shared
+// memory fits twice; left to itself the compiler uses ~156 registers at
+// Nx = 1024 and only one CTA fits: 141 vs 152 us per launch); larger rows
+// keep one CTA.
+__global__ void __launch_bounds__(TARA_ROW_LB(11 * (M / P)), (11 * (M / P) <= 352 ? 2 : 1))
+    k_row_coh(const RowCohArgs<T> a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   row_coh_rows<T, M, P>(a, blockIdx.x * a.rb, reinterpret_cast<Cx<T>*>(smraw));
 }
