@@ -163,6 +163,23 @@ typedef struct {
 } tara_ic;
 int tara_set_state_random(tara_session* s, const tara_ic* ic);
 
+/* ---- tracer particles (src/main2csh.f95:93-96, 187-268), vorticity models ----
+ * np particles at (xp, yp) (host arrays, updated in place).  nsteps > 0:
+ * nsteps times, one step of the state (stepper) and then, as the driver does,
+ * one forward-Euler move of every particle by dt with the velocity of the new
+ * state, positions wrapped into (0, Lx] x (0, Ly].  nsteps = 0: only the
+ * velocities at the particles.  vxp, vyp (may be NULL) receive the last
+ * velocities; a position that is not finite gets NaN velocities and stays.
+ * Velocity: u = c2r(i ky psi_k)/(NxNy), v = c2r(-i kx psi_k)/(NxNy),
+ * psi_k = omega_k/(k^2 + lambda) (lambda = 0 for csh), interpolated
+ * bilinearly in the particle's grid cell with the reference's formula and
+ * operation order (no fused multiply-add); in the last column / row the far
+ * corner is x = Lx / y = Ly as in the reference, and the far grid values are
+ * those of column / row 1 (the reference reads past its arrays there).
+ * Other models: TARA_EUNSUPPORTED. */
+int tara_tracers_run(tara_session* s, int stepper, int nsteps, int np, double* xp, double* yp, double* vxp,
+                     double* vyp);
+
 /* ---- binary checkpoint / restart (no counterpart in the reference, whose
  * drivers always start from an initial condition: src/main2com.f95:215-343,
  * src/main2coh.f95:176-257) ----

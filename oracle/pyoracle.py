@@ -268,3 +268,60 @@ def spectrum_com(Nx, Ny, P: ComParams, state, pi=PI):
     out = np.zeros(n)
     lib().ora_spectrum_com(Nx, Ny, pi, C.byref(P), _ptr_array(st), n, _p(out))
     return out
+
+
+# ---------------------------------------------------------------- tracers
+def vort_velocity_real(omegak: np.ndarray, Nx: int, Ny: int, Lx: float, Ly: float, pi: float, lam: float = 0.0):
+    """Real (ux, uy) of a vorticity spectrum as src/main2csh.f95:122-173 forms
+    them: psi = omega/(kx^2 + ky^2 [+ lambda]) (0 at k = 0), ukx = i ky psi,
+    uky = -i kx psi, c2r (the reference's FFTW) / (Nx Ny)."""
+    Nh = Nx // 2 + 1
+    kx = 2.0 * pi * np.arange(Nh, dtype=np.float64) / Lx
+    j = np.arange(Ny, dtype=np.float64)
+    ky = np.where(np.arange(Ny) < Ny // 2, 2.0 * pi * j / Ly, 2.0 * pi * (j - Ny) / Ly)
+    KX, KY = np.meshgrid(kx, ky)
+    den = KX * KX + KY * KY + lam
+    den[0, 0] = 1.0
+    psi = omegak / den
+    psi[0, 0] = 0.0
+    ux = c2r_2d(1j * KY * psi, Nx) / (Nx * Ny)
+    uy = c2r_2d(-1j * KX * psi, Nx) / (Nx * Ny)
+    return ux, uy
+
+
+def _tracer_cell(p, d, L, N):
+    m = np.trunc(p / d).astype(np.int64) + 1          # aint(p/d) + 1
+    m = np.clip(m, 1, N + 1)
+    p0 = (m - 1).astype(np.float64) * d              # x(m)
+    p1 = np.where(m == N, L, m.astype(np.float64) * d)   # x(m+1), Lx in the last column
+    return (m - 1) % N, m % N, p0, p1
+
+
+def tracer_velocity(ux, uy, xp, yp, Lx, Ly):
+    """Bilinear velocity at (xp, yp) in (0, Lx] x (0, Ly] (src/main2csh.f95:187-242,
+    products and sums in the reference's order); in the last column / row the
+    far grid values are those of column / row 1 (periodic)."""
+    Ny, Nx = ux.shape
+    dx, dy = Lx / float(Nx), Ly / float(Ny)
+    h = 1.0 / (dx * dy)
+    i0, i1, x0, x1 = _tracer_cell(xp, dx, Lx, Nx)
+    j0, j1, y0, y1 = _tracer_cell(yp, dy, Ly, Ny)
+    ax, bx, ay, by = x1 - xp, xp - x0, y1 - yp, yp - y0
+
+    def interp(u):
+        v = u[j0, i0] * ax * ay * h
+        v = v + u[j0, i1] * bx * ay * h
+        v = v + u[j1, i0] * ax * by * h
+        return v + u[j1, i1] * bx * by * h
+    return interp(ux), interp(uy)
+
+
+def tracer_move(xp, yp, vx, vy, dt, Lx, Ly):
+    """One forward-Euler move with the wrap of src/main2csh.f95:244-256."""
+    xn = xp + vx * dt
+    yn = yp + vy * dt
+    xn = xn - np.trunc(xn / Lx).astype(np.int64).astype(np.float64) * Lx
+    xn = np.where(xn <= 0.0, xn + Lx, xn)
+    yn = yn - np.trunc(yn / Ly).astype(np.int64).astype(np.float64) * Ly
+    yn = np.where(yn <= 0.0, yn + Ly, yn)
+    return xn, yn

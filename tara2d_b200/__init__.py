@@ -123,6 +123,7 @@ def lib():
         L.tara_write_snapshot.argtypes = [P, C.c_char_p]
         L.tara_checkpoint_write.argtypes = [P, C.c_char_p, C.c_longlong, D]
         L.tara_set_state_random.argtypes = [P, C.POINTER(IcDesc)]
+        L.tara_tracers_run.argtypes = [P, I, I, I, P, P, P, P]
         L.tara_checkpoint_read.argtypes = [P, C.c_char_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
         L.tara_format_list_directed.argtypes = [P, I, C.c_char_p, I]
         L.tara_ens_open.argtypes = [C.POINTER(C.c_void_p), I, I, P, C.POINTER(Params), I]
@@ -274,6 +275,21 @@ class Session:
         initial.hashed_state builds the same state."""
         d = IcDesc(kind=kind, seed=seed, k0=k0, e1=e1, e2=e2, kmin=kmin, kmax=kmax)
         check(lib().tara_set_state_random(self._h, C.byref(d)), "tara_set_state_random")
+
+    def tracers_run(self, stepper: int, nsteps: int, xp, yp):
+        """Tracer particles (vorticity models): nsteps state steps, each followed
+        by one Euler move of the particles with the new velocity; xp, yp are
+        float64 arrays updated in place.  Returns the last velocities (vx, vy)."""
+        for a in (xp, yp):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+                raise TaraError("tracer positions must be contiguous float64 arrays")
+        n = int(xp.size)
+        if yp.size != n:
+            raise TaraError("xp and yp differ in length")
+        vx, vy = np.zeros(n), np.zeros(n)
+        check(lib().tara_tracers_run(self._h, stepper, nsteps, n, xp.ctypes.data, yp.ctypes.data, vx.ctypes.data,
+                                     vy.ctypes.data), "tara_tracers_run")
+        return vx, vy
 
     def checkpoint(self, path: str, step: int = 0, time: float = 0.0) -> None:
         """Binary checkpoint of state, history, parameters, step and time

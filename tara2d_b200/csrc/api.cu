@@ -12,6 +12,7 @@
 #include "diag.cuh"
 #include "output.h"
 #include "ic.cuh"
+#include "tracers.cuh"
 #include "realspace.cuh"
 #include "session.h"
 
@@ -571,6 +572,56 @@ struct SessionT : tara_session {
     return device_status();
   }
 
+  int tracers_run(int stepper, int nsteps, int np, double* xp, double* yp, double* vxp, double* vyp) override {
+    if (model != TARA_MODEL_CSH && model != TARA_MODEL_CSS) {
+      set_error("tracer particles move with the velocity of the vorticity models");
+      return TARA_EUNSUPPORTED;
+    }
+    if (np < 0 || nsteps < 0 || (np > 0 && (!xp || !yp))) { set_error("bad tracer arguments"); return TARA_EINVAL; }
+    if (np == 0) return step(stepper, nsteps);
+    TARA_TRY(ensure_real());
+    if (workpool().count < 4) { set_error("work pool too small"); return TARA_EINVAL; }
+    const size_t nn = (size_t)Nx * Ny;
+    T* ux = rbuf + nn;  // real fields 1 and 2 of nf + 3 >= 4
+    T* uy = rbuf + 2 * nn;
+    Cx<T>* wk[4] = {workpool()[0], workpool()[1], workpool()[2], workpool()[3]};
+    double* d = nullptr;
+    if (cudaMalloc(&d, 4 * (size_t)np * sizeof(double)) != cudaSuccess) {
+      set_error("cudaMalloc of the tracer arrays failed");
+      return TARA_ENOMEM;
+    }
+    double *dx = d, *dy = d + np, *dvx = d + 2 * (size_t)np, *dvy = d + 3 * (size_t)np;
+    const T lam = model == TARA_MODEL_CSS ? vortp.lambda : (T)0;
+    int r = TARA_OK;
+    if (cudaMemcpyAsync(dx, xp, np * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(dy, yp, np * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+      set_error("tracer upload failed");
+      r = TARA_ECUDA;
+    }
+    if (r == TARA_OK && nsteps == 0) {
+      r = tracer_velocity_real<T>(g, u[0], lam, ux, uy, wk, st);
+      if (r == TARA_OK) r = tracers_update<T>(g, ux, uy, np, dx, dy, dvx, dvy, p.dt, false, st);
+    }
+    for (int k = 0; k < nsteps && r == TARA_OK; k++) {
+      r = step(stepper, 1);  // the new state is u
+      if (r == TARA_OK) r = tracer_velocity_real<T>(g, u[0], lam, ux, uy, wk, st);
+      if (r == TARA_OK) r = tracers_update<T>(g, ux, uy, np, dx, dy, dvx, dvy, p.dt, true, st);
+    }
+    if (r == TARA_OK) {
+      const size_t b = np * sizeof(double);
+      if (cudaMemcpyAsync(xp, dx, b, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaMemcpyAsync(yp, dy, b, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          (vxp && cudaMemcpyAsync(vxp, dvx, b, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
+          (vyp && cudaMemcpyAsync(vyp, dvy, b, cudaMemcpyDeviceToHost, st) != cudaSuccess)) {
+        set_error("tracer download failed");
+        r = TARA_ECUDA;
+      }
+    }
+    cudaStreamSynchronize(st);
+    cudaFree(d);
+    return r == TARA_OK ? device_status() : r;
+  }
+
   int num_shells() override { return diag_num_shells(Nx, Ny, p.Lx, p.Ly, p.pi); }
   int record(double* drec) {
     h_for = nullptr;  // the diagnostics use the work pool
@@ -795,6 +846,10 @@ int tara_set_state_real(tara_session* s, const double* const* fields) {
 }
 int tara_set_state_random(tara_session* s, const tara_ic* ic) {
   return s ? s->fail_if(s->set_state_random(ic)) : TARA_EINVAL;
+}
+int tara_tracers_run(tara_session* s, int stepper, int nsteps, int np, double* xp, double* yp, double* vxp,
+                     double* vyp) {
+  return s ? s->fail_if(s->tracers_run(stepper, nsteps, np, xp, yp, vxp, vyp)) : TARA_EINVAL;
 }
 
 // The drivers' grid files: one line per grid point, x outer, y inner, as

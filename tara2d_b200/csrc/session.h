@@ -46,6 +46,10 @@ struct tara_session {
   virtual int set_state_real(const double* const* h) = 0;
   // the state from a seeded initial condition built on the device
   virtual int set_state_random(const tara_ic* ic) = 0;
+  // tracer particles (host arrays of np): nsteps steps of the state, each
+  // followed by one particle move with the new state's velocity (nsteps = 0:
+  // only the velocities at the particles)
+  virtual int tracers_run(int stepper, int nsteps, int np, double* xp, double* yp, double* vxp, double* vyp) = 0;
   // nrec diagnostics records of the state, one before the first step and one
   // after every `every` steps (nsteps = (nrec - 1) * every), into rec
   // (host, nrec * (TARA_DIAG_VALUES + num_shells()) doubles)
