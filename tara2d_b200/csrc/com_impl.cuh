@@ -87,7 +87,10 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
   // flux q at one point                                                (:105-106, :193-213)
   const T cs2 = a.cs2;
   auto flux = [&](int qq, T rho, T mx, T my, T E, T bx, T by) -> T {
-    const T ux = mx / rho, uy = my / rho;
+    // u = (rho u)/rho through one reciprocal (the reference divides twice;
+    // the results differ in the last bit)
+    const T ir = (T)1 / rho;
+    const T ux = mx * ir, uy = my * ir;
     const T B2 = bx * bx + by * by;
     const T Pr = cs2 * rho;
     switch (qq) {
