@@ -251,8 +251,9 @@ k_row_com2(const RowCom2Args<T> a) {
   for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
     if (!FIX) {
       // d_Bx_dy = d_ux_dx/(NxNy), d_By_dx = d_uy_dy/(NxNy)   (reference defect)
+      // (/ NxNy: an exact multiply when NxNy is a power of two)
       const Cx<T> p = dux[n], q = duy[n];
-      curl[n] = cx<T>(q.x / tb.nn - p.x / tb.nn, q.y / tb.nn - p.y / tb.nn);
+      curl[n] = cx<T>(normalise(q.x, tb) - normalise(p.x, tb), normalise(q.y, tb) - normalise(p.y, tb));
     } else {
       const Cx<T> p = curl[n], q = aux[n];
       curl[n] = cx<T>(p.x - q.x, p.y - q.y);
