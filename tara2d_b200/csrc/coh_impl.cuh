@@ -96,9 +96,10 @@ __device__ __forceinline__ void row_coh_rows(const RowCohArgs<T>& a, int y0, Cx<
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       const T n = q[0][h], ux = q[1][h], uy = q[2][h];
+      const T in = (T)1 / n;  // one reciprocal for the four divisions by n (last-bit differences)
       o[0][h] = ux * q[3][h] + uy * q[4][h] + n * (q[5][h] + q[8][h]);
-      o[1][h] = (ux * q[5][h] + uy * q[6][h]) + q[9][h] / n + cs2 * (q[3][h] / n);
-      o[2][h] = (ux * q[7][h] + uy * q[8][h]) + q[10][h] / n + cs2 * (q[4][h] / n);
+      o[1][h] = (ux * q[5][h] + uy * q[6][h]) + q[9][h] * in + cs2 * (q[3][h] * in);
+      o[2][h] = (ux * q[7][h] + uy * q[8][h]) + q[10][h] * in + cs2 * (q[4][h] * in);
     }
 #pragma unroll
     for (int f = 0; f < 3; f++) arr(f)[m] = cx<T>(o[f][0], o[f][1]);
