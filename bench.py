@@ -363,7 +363,8 @@ def main():
     achieved = bytes_launch / (avg_ms / 1e3) / 1e9
     traffic = load_ncu_traffic().get(dname, {}).get("dram_bytes_per_launch")
     roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "frac": achieved / peak, "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                                else "fallback (MEASURED_PEAKS.json absent; earlier copy measurement, 6650 GB/s)"),
                 "traffic": traffic, "avg_launch_ms": avg_ms,
                 "kernels": {k: {"ms_per_launch": v[0] / v[1], "launches": v[1],
                                 "share": v[0] / max(prof_total, 1e-9),

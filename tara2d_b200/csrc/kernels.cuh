@@ -79,8 +79,10 @@ template <class T> __device__ __forceinline__ T ksq(T kx, T ky) { return mul_rn(
 template <class T>
 __device__ __forceinline__ Cx<T> apply_psi_mul(int mul, T lam, T kx, T ky, bool origin, Cx<T> w) {
   const T k2 = ksq(kx, ky);
-  const T den = k2 + lam;
-  const Cx<T> psi = origin ? cx<T>(0, 0) : cx<T>(w.x / den, w.y / den);
+  // one reciprocal of k^2 + lam per mode (the reference divides both
+  // components; the results differ in the last bit)
+  const T iden = (T)1 / (k2 + lam);
+  const Cx<T> psi = origin ? cx<T>(0, 0) : cx<T>(w.x * iden, w.y * iden);
   switch (mul) {
     case MUL_PSI: return psi;
     case MUL_IKY_PSI: return ikmul(ky, psi);
