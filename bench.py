@@ -255,6 +255,81 @@ def run_ensemble(args):
     return 0
 
 
+# ------------------------------------------------------------------ 3D MHD
+def mhd3_bytes_per_step(N):
+    """Algorithmic bytes of one 3D AB2 step at N^3 (every field each kernel must
+    read or write once): 224 S + 74 R, S = spectral field (Nh N N complex128),
+    R = real field (N^3 float64).  c2r of 8 fields 40 S + 8 R, velocity 7 R,
+    r2c of 3 fields 15 S + 3 R, c2r of 9 derivative fields 45 S + 9 R, fluxes
+    32 R, r2c of 15 fluxes 75 S + 15 R, assembly + AB2 49 S."""
+    S = (N // 2 + 1) * N * N * 16
+    R = N ** 3 * 8
+    return 224 * S + 74 * R
+
+
+def run_mhd3d(args):
+    """Side workload (not the headline): the 3D path of src/derive3com.f95 +
+    src/ab3com.f95 (the driver's AB2 loop, src/main3com.f95:536-600) at N^3 FP64,
+    N = --grid3 (256 by default), on one GPU."""
+    import tara2d_b200 as T
+    from tara2d_b200 import initial
+    N = args.grid3
+    T.set_device(0)
+    prm = dict(pi=PI, Lx=2 * PI, Ly=2 * PI, Lz=2 * PI, mu=0.01, CS=10.0, eta=0.005, dt=1e-4)
+    st0 = initial.mhd3_state(N, N, N, seed=0, noise=1e-4)
+    W, K = max(3, args.warmup), max(1, args.steps)
+    peak, peak_kind = peaks()
+    with T.Mhd3(N, N, N, T.Params3D.make(**prm)) as s:
+        s.set_state(st0)
+        s.step(W)
+        clk = ClockSampler(T.device_pci_bus_id())
+        clk.start()
+        ms = s.time_steps(K)
+        clocks = clk.stop()
+        # e2e: per step the state from host memory, one step, the state back
+        E = max(1, min(args.e2e_steps, 10))
+        host = [np.ascontiguousarray(a) for a in st0]
+        t0 = time.perf_counter()
+        for _ in range(E):
+            s.set_state(host)
+            s.step(1)
+            host = s.get_state()
+        e2e_s = (time.perf_counter() - t0) / E
+        launches = s.launches_per_step()
+    bps = mhd3_bytes_per_step(N)
+    per_s = K / (ms / 1e3)
+    field = (N // 2 + 1) * N * N * 16
+    out = {"metric": f"3D MHD AB2 steps/s at {N}^3 (src/derive3com.f95 + src/ab3com.f95)", "value": per_s,
+           "unit": "steps/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"3D compressible MHD (*3com), {N}^3, FP64, AB2 dt=1e-4, mu=0.01, CS=10, "
+                                  "eta=0.005, smooth fields + 1e-4 noise (seed 0)",
+                      "grid": [N, N, N],
+                      "l2": f"working set {(42 * field + 35 * N ** 3 * 8) / 1e9:.1f} GB > 126 MB L2; no flush"},
+           "grid_point_steps_per_s": per_s * N ** 3,
+           "e2e": {"value": 1.0 / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 8 * field,
+                   "d2h_bytes_per_step": 8 * field,
+                   "note": "per step: tara3d_set_state from host, tara3d_step(1), tara3d_get_state"},
+           "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": bps * per_s / 1e9, "peak": peak,
+                        "unit": "GB/s", "frac": bps * per_s / 1e9 / peak, "bytes_per_step": bps,
+                        "traffic": None, "peak_source": peak_kind,
+                        "note": "224 S + 74 R per AB2 step (every field each kernel reads or writes, once)"},
+           "clocks": clocks, "gpu_launches": launches * K}
+    if not args.no_cpu_baseline:
+        from oracle import pyoracle as O  # the checker, timed as the CPU baseline only
+        P = O.Com3Params(Lx=2 * PI, Ly=2 * PI, Lz=2 * PI, mu=0.01, CS=10.0, eta=0.005, dt=1e-4)
+        t0 = time.perf_counter()
+        O.run3com(N, N, N, P, 1, st0)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "steps/s", "cores": O.lib().ora_get_threads(),
+                               "kind": "port",
+                               "sample": f"1 AB2 step at {N}^3 (C restatement of src/derive3com.f95 + "
+                                         "src/ab3com.f95 over the reference's FFTW 3.3.9, OpenMP pointwise "
+                                         "loops, single-threaded FFTs)"}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ ranks
 class Ranks:
     """One process per GPU (replicas: the path does not shard).  Rank and
@@ -313,8 +388,10 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=1024, help="grid size (profiling runs only; the metric is at 1024)")
-    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble"],
-                    help="mhd1024: the headline; ensemble: the 256-run batched side workload")
+    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "mhd3d"],
+                    help="mhd1024: the headline; ensemble: the 256-run batched side workload; "
+                         "mhd3d: the 3D path at --grid3^3")
+    ap.add_argument("--grid3", type=int, default=256, help="3D grid size of --workload mhd3d")
     args = ap.parse_args()
     global N
     N = args.grid
@@ -322,6 +399,8 @@ def main():
         return run_reference(args)
     if args.workload == "ensemble":
         return run_ensemble(args)
+    if args.workload == "mhd3d":
+        return run_mhd3d(args)
 
     ranks = Ranks("nccl")
     world, rank, local = ranks.world, ranks.rank, ranks.local

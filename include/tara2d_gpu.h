@@ -398,8 +398,70 @@ int tara_set_legacy_mode(int mode);
 
 /* COMMON /comm/ storage used by the drop-in entry points (11 doubles:
  * hydro units read Lx,Ly,mux,muy,ms,CS,dt; MHD units read
- * Lx,Ly,spheat,mu,ms,CS,mu_0,eta,dt,kf,A). */
+ * Lx,Ly,spheat,mu,ms,CS,mu_0,eta,dt,kf,A).  The 3D MHD units read the 3D
+ * driver's block (src/main3com.f95:56): two integer(4) (iret, thread_num) in
+ * the first 8 bytes, then time_max,Lx,Ly,Lz,dx,dy,dz,spheat,mu,ms,CS,mu_0,
+ * eta,dt,kf as comm_[1..15]. */
 extern double comm_[16];
+
+/* ---------------------------------------------------------------------------
+ * 3D compressible MHD (src/derive3com.f95:5-1047, src/ab3com.f95:6-66), FP64.
+ *
+ * Spectral fields are the reference's complex(8) (Nh,Ny,Nz) arrays,
+ * Nh = Nx/2+1, as interleaved (re, im) doubles; the 8 fields are, in order,
+ * rho, rho ux, rho uy, rho uz, E, Bx, By, Bz.  Nx, Ny, Nz in
+ * {16, 32, 64, 128, 256, 512}.  The reference's constants are kept: the
+ * momentum and induction equations diffuse with 1/450 (not mu), the energy
+ * equation adds mu (div u)^2, eta enters only the energy flux, and ab3com
+ * leaves E unchanged.
+ * ------------------------------------------------------------------------- */
+typedef struct tara3d tara3d;
+typedef struct {
+  double pi, Lx, Ly, Lz;  /* box lengths as the reference holds them (already times pi) */
+  double mu, CS, eta, dt; /* COMMON /comm/ mu, CS, eta, dt of src/main3com.f95:56 */
+  double reserved[8];
+} tara3d_params;
+
+/* One device-resident 3D state; AB2 history starts at zero (the reference's
+ * d_*_dt_old before the first step). */
+int tara3d_open(tara3d** out, int Nx, int Ny, int Nz, const tara3d_params* p);
+int tara3d_close(tara3d* s);
+int tara3d_set_params(tara3d* s, const tara3d_params* p);
+/* host <-> device, 8 fields of Nh*Ny*Nz complex(8) each */
+int tara3d_set_state(tara3d* s, const double* const fields[8]);
+int tara3d_get_state(tara3d* s, double* const fields[8]);
+int tara3d_set_history(tara3d* s, const double* const d_old[8]);
+/* derive3com of the current state into host arrays (state unchanged) */
+int tara3d_rhs(tara3d* s, double* const d_new[8]);
+/* nsteps of derive3com + ab3com + history shift (src/main3com.f95:548-600) */
+int tara3d_step(tara3d* s, int nsteps);
+/* the same, timed on the device with CUDA events (milliseconds in *ms) */
+int tara3d_time_steps(tara3d* s, int nsteps, float* ms);
+/* kernel launches of one step */
+int tara3d_launches_per_step(tara3d* s);
+
+/* Drop-in replacements (gfortran names) of the 3D subroutines; parameters
+ * from comm_ as laid out above.  Status in tara_legacy_status(). */
+void derive3com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nz, const int32_t* Nh,
+                 const double* pi, const double* time, double* rho_k, double* rho_ux_k,
+                 double* rho_uy_k, double* rho_uz_k, double* E_k, double* Bx_k, double* By_k,
+                 double* Bz_k, double* d_rho_k_dt_old, double* d_rho_k_dt_new,
+                 double* d_rho_ux_k_dt_old, double* d_rho_ux_k_dt_new, double* d_rho_uy_k_dt_old,
+                 double* d_rho_uy_k_dt_new, double* d_rho_uz_k_dt_old, double* d_rho_uz_k_dt_new,
+                 double* d_E_k_dt_old, double* d_E_k_dt_new, double* d_Bx_k_dt_old,
+                 double* d_Bx_k_dt_new, double* d_By_k_dt_old, double* d_By_k_dt_new,
+                 double* d_Bz_k_dt_old, double* d_Bz_k_dt_new);
+void ab3com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nz, const int32_t* Nh,
+             const double* pi, const double* time, double* rho_k, double* rho_ux_k, double* rho_uy_k,
+             double* rho_uz_k, double* E_k, double* Bx_k, double* By_k, double* Bz_k,
+             double* rho_k_new, double* rho_ux_k_new, double* rho_uy_k_new, double* rho_uz_k_new,
+             double* E_k_new, double* Bx_k_new, double* By_k_new, double* Bz_k_new,
+             double* d_rho_k_dt_old, double* d_rho_k_dt_new, double* d_rho_ux_k_dt_old,
+             double* d_rho_ux_k_dt_new, double* d_rho_uy_k_dt_old, double* d_rho_uy_k_dt_new,
+             double* d_rho_uz_k_dt_old, double* d_rho_uz_k_dt_new, double* d_E_k_dt_old,
+             double* d_E_k_dt_new, double* d_Bx_k_dt_old, double* d_Bx_k_dt_new,
+             double* d_By_k_dt_old, double* d_By_k_dt_new, double* d_Bz_k_dt_old,
+             double* d_Bz_k_dt_new);
 
 #ifdef __cplusplus
 }

@@ -34,6 +34,12 @@ class ComParams(C.Structure):
                [("fix_curlB", C.c_int)]
 
 
+class Com3Params(C.Structure):
+    """3D MHD: Lx, Ly, Lz (already times pi) and mu, CS, eta, dt of COMMON /comm/
+    (src/main3com.f95:56)."""
+    _fields_ = [(n, C.c_double) for n in ("Lx", "Ly", "Lz", "mu", "CS", "eta", "dt")]
+
+
 def build() -> None:
     """Build the oracle (and, with the reference checkout present, its FFTW)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
@@ -71,6 +77,9 @@ def lib():
         L.ora_num_shells.restype = i
         L.ora_spectrum_coh.argtypes = [i, i, d, C.POINTER(CohParams), P, P, i, P]
         L.ora_spectrum_com.argtypes = [i, i, d, C.POINTER(ComParams), P, i, P]
+        L.ora_derive3com.argtypes = [i, i, i, d, C.POINTER(Com3Params), P, P]
+        L.ora_ab3com.argtypes = [i, i, i, d, P, P, P, P]
+        L.ora_run3com.argtypes = [i, i, i, d, C.POINTER(Com3Params), i, P, P]
         L.ora_set_threads.argtypes = [i]
         L.ora_get_threads.restype = i
     return _lib
@@ -325,3 +334,35 @@ def tracer_move(xp, yp, vx, vy, dt, Lx, Ly):
     yn = yn - np.trunc(yn / Ly).astype(np.int64).astype(np.float64) * Ly
     yn = np.where(yn <= 0.0, yn + Ly, yn)
     return xn, yn
+
+
+# ------------------------------------------------------------------ 3D MHD
+def derive3com(Nx, Ny, Nz, P: Com3Params, state, pi=PI):
+    """src/derive3com.f95:5-1047: d/dt of (rho, rho ux, rho uy, rho uz, E, Bx, By, Bz),
+    each a complex (Nz, Ny, Nx/2+1) array (the Fortran (Nh,Ny,Nz) layout)."""
+    Nh = Nx // 2 + 1
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    out = [_cz((Nz, Ny, Nh)) for _ in range(8)]
+    lib().ora_derive3com(Nx, Ny, Nz, pi, C.byref(P), _ptr_array(st), _ptr_array(out))
+    return out
+
+
+def ab3com(Nx, Ny, Nz, dt, state, d_old, d_new):
+    """src/ab3com.f95:44-61 (E unchanged)."""
+    Nh = Nx // 2 + 1
+    st = [np.ascontiguousarray(a, dtype=np.complex128) for a in state]
+    do = [np.ascontiguousarray(a, dtype=np.complex128) for a in d_old]
+    dn = [np.ascontiguousarray(a, dtype=np.complex128) for a in d_new]
+    out = [_cz((Nz, Ny, Nh)) for _ in range(8)]
+    lib().ora_ab3com(Nx, Ny, Nz, dt, _ptr_array(st), _ptr_array(out), _ptr_array(do), _ptr_array(dn))
+    return out
+
+
+def run3com(Nx, Ny, Nz, P: Com3Params, nsteps, state, d_old=None, pi=PI):
+    """nsteps of the time loop of src/main3com.f95:536-600 (AB2, history from zero)."""
+    Nh = Nx // 2 + 1
+    st = [np.array(a, dtype=np.complex128, order="C") for a in state]
+    do = [np.array(a, dtype=np.complex128, order="C") for a in d_old] if d_old is not None else \
+        [_cz((Nz, Ny, Nh)) for _ in range(8)]
+    lib().ora_run3com(Nx, Ny, Nz, pi, C.byref(P), nsteps, _ptr_array(st), _ptr_array(do))
+    return st, do

@@ -837,3 +837,162 @@ void ora_spectrum_com(int Nx, int Ny, double pi, const ora_com_params *P, const 
   shell_spectrum(Nx, Ny, pi, P->Lx, P->Ly, uxk, uyk, nbins, Ek);
   fftw_free(rho); fftw_free(ux); fftw_free(uy); fftw_free(uxk); fftw_free(uyk);
 }
+
+/* ======================================================================= */
+/* 3D MHD: derive3com (src/derive3com.f95:5-1047), ab3com (src/ab3com.f95)   */
+/* ======================================================================= */
+/* Fortran (Nx,Ny,Nz) is C [Nz][Ny][Nx]: dfftw_plan_dft_c2r_3d(p,Nx,Ny,Nz,...)
+ * is fftw_plan_dft_c2r_3d(Nz,Ny,Nx,...) (lib/fftw/api/f77funcs.h). */
+static void c2r3_destroy(int Nx, int Ny, int Nz, ocplx *in, double *out) {
+  fftw_plan p = fftw_plan_dft_c2r_3d(Nz, Ny, Nx, (fftw_complex *)in, out, FFTW_ESTIMATE);
+  fftw_execute(p);
+  fftw_destroy_plan(p);
+}
+static void r2c3(int Nx, int Ny, int Nz, const double *in, ocplx *out) {
+  fftw_plan p = fftw_plan_dft_r2c_3d(Nz, Ny, Nx, (double *)in, (fftw_complex *)out, FFTW_ESTIMATE);
+  fftw_execute(p);
+  fftw_destroy_plan(p);
+}
+
+void ora_derive3com(int Nx, int Ny, int Nz, double pi, const ora_com3_params *P, const ocplx *const st[8],
+                    ocplx *const dnew[8]) {
+  const int Nh = Nx / 2 + 1;
+  const size_t nc = (size_t)Nh * Ny * Nz, nr = (size_t)Nx * Ny * Nz;
+  const double NN = (double)Nx * (double)Ny * (double)Nz; /* dfloat(Nx)*dfloat(Ny)*dfloat(Nz) */
+  double *R[8], *U[3], *Dv[9], *F[19];
+  ocplx *tmp = (ocplx *)xmalloc(sizeof(ocplx) * nc), *uk[3], *Fk[19];
+  for (int q = 0; q < 8; q++) R[q] = (double *)xmalloc(sizeof(double) * nr);
+  for (int q = 0; q < 3; q++) { U[q] = (double *)xmalloc(sizeof(double) * nr); uk[q] = (ocplx *)xmalloc(sizeof(ocplx) * nc); }
+  for (int q = 0; q < 9; q++) Dv[q] = (double *)xmalloc(sizeof(double) * nr);
+  for (int q = 0; q < 19; q++) { F[q] = (double *)xmalloc(sizeof(double) * nr); Fk[q] = (ocplx *)xmalloc(sizeof(ocplx) * nc); }
+  /* state c2r from *_dum copies (:60-135) */
+  for (int q = 0; q < 8; q++) {
+    memcpy(tmp, st[q], sizeof(ocplx) * nc);
+    c2r3_destroy(Nx, Ny, Nz, tmp, R[q]);
+  }
+  /* normalisation and velocity (:160-182); the forcing (:184-188) is not used */
+  OMP_FOR
+  for (size_t p = 0; p < nr; p++) {
+    for (int q = 0; q < 8; q++) R[q][p] = R[q][p] / NN;
+    U[0][p] = R[1][p] / R[0][p];
+    U[1][p] = R[2][p] / R[0][p];
+    U[2][p] = R[3][p] / R[0][p];
+  }
+  for (int q = 0; q < 3; q++) r2c3(Nx, Ny, Nz, U[q], uk[q]); /* (:198-215) */
+  /* first derivatives (:232-340): i kx ux, i ky uy, i kz uz, i ky Bx, i kz Bx,
+   * i kx By, i kz By, i kx Bz, i ky Bz */
+  const ocplx *dsrc[9] = {uk[0], uk[1], uk[2], st[5], st[5], st[6], st[6], st[7], st[7]};
+  const int dk[9] = {0, 1, 2, 1, 2, 0, 2, 0, 1};
+  for (int q = 0; q < 9; q++) {
+    OMP_FOR
+    for (int k = 0; k < Nz; k++)
+      for (int j = 0; j < Ny; j++)
+        for (int i = 0; i < Nh; i++) {
+          const double kx = kx_of(i, pi, P->Lx), ky = ky_of(j, Ny, pi, P->Ly), kz = ky_of(k, Nz, pi, P->Lz);
+          const double kk = dk[q] == 0 ? kx : (dk[q] == 1 ? ky : kz);
+          const size_t m = (size_t)i + (size_t)Nh * ((size_t)j + (size_t)Ny * k);
+          tmp[m] = ik_mul(kk, dsrc[q][m]);
+        }
+    c2r3_destroy(Nx, Ny, Nz, tmp, Dv[q]);
+  }
+  /* real-space fluxes (:343-414) */
+  const double CS = P->CS, eta = P->eta;
+  OMP_FOR
+  for (size_t p = 0; p < nr; p++) {
+    for (int q = 0; q < 9; q++) Dv[q][p] = Dv[q][p] / NN;
+    const double rho = R[0][p], rux = R[1][p], ruy = R[2][p], ruz = R[3][p], E = R[4][p];
+    const double Bx = R[5][p], By = R[6][p], Bz = R[7][p];
+    const double ux = U[0][p], uy = U[1][p], uz = U[2][p];
+    const double B2 = Bx * Bx + By * By + Bz * Bz;
+    const double cxB = Dv[8][p] - Dv[6][p], cyB = Dv[7][p] - Dv[4][p], czB = Dv[5][p] - Dv[3][p];
+    const double Pp = CS * CS * rho;
+    F[0][p] = rux * ux + Pp + B2 / 2.0 - Bx * Bx;
+    F[1][p] = rux * uy - Bx * By;
+    F[2][p] = rux * uz - Bx * Bz;
+    F[3][p] = rux * uy - Bx * By; /* Mom_y_1 as written */
+    F[4][p] = ruy * uy + Pp + B2 / 2.0 - By * By;
+    F[5][p] = ruy * uz - By * Bz;
+    F[6][p] = ruz * ux - Bz * Bx;
+    F[7][p] = ruz * uy - Bz * By;
+    F[8][p] = ruz * uz + Pp + B2 / 2.0 - Bz * Bz;
+    F[9][p] = (E + Pp + B2 / 2.0) * ux - ux * Bx * Bx - uy * Bx * By - uz * Bx * Bz - eta * (By * czB + Bz * cyB);
+    F[10][p] = (E + Pp + B2 / 2.0) * uy - ux * Bx * By - uy * By * By - uz * By * Bz + eta * (Bx * czB - Bz * cxB);
+    F[11][p] = (E + Pp + B2 / 2.0) * uz - ux * Bz * Bx - uy * Bz * By - uz * Bz * Bz + eta * (Bx * cyB + By * cxB);
+    const double dv = Dv[0][p] + Dv[1][p] + Dv[2][p];
+    F[12][p] = dv * dv;
+    F[13][p] = ux * By - uy * Bx;
+    F[14][p] = ux * Bz - uz * Bx;
+    F[15][p] = ux * By - uy * Bx; /* Mag_y_1 as written */
+    F[16][p] = uy * Bz - uz * By;
+    F[17][p] = ux * Bz - uz * Bx; /* Mag_z_1 as written */
+    F[18][p] = uy * Bz - uz * By; /* Mag_z_2 as written */
+  }
+  for (int q = 0; q < 19; q++) r2c3(Nx, Ny, Nz, F[q], Fk[q]); /* (:416-500) */
+  /* spectral derivatives, mask and sums (:502-1043) */
+  const double thr = ((double)(Nx + Ny + Nz) / 3.0) / 3.0 + 0;
+  const double mu = P->mu;
+  OMP_FOR
+  for (int k = 0; k < Nz; k++)
+    for (int j = 0; j < Ny; j++)
+      for (int i = 0; i < Nh; i++) {
+        const size_t m = (size_t)i + (size_t)Nh * ((size_t)j + (size_t)Ny * k);
+        const double kx = kx_of(i, pi, P->Lx), ky = ky_of(j, Ny, pi, P->Ly), kz = ky_of(k, Nz, pi, P->Lz);
+        if (sqrt(kx * kx + ky * ky + kz * kz) >= thr) {
+          for (int q = 0; q < 8; q++) dnew[q][m] = 0;
+          continue;
+        }
+        ocplx v3[3];
+        for (int c = 0; c < 3; c++) {
+          const ocplx u = uk[c][m];
+          v3[c] = rmul(kx * kx, u) + rmul(ky * ky, u) + rmul(kz * kz, u);
+          v3[c] = CMPLX(creal(v3[c]) / 450.0, cimag(v3[c]) / 450.0);
+        }
+        ocplx vb[3];
+        for (int c = 0; c < 3; c++) {
+          const ocplx b = st[5 + c][m];
+          vb[c] = rmul(kx * kx, b) + rmul(ky * ky, b) + rmul(kz * kz, b);
+          vb[c] = CMPLX(creal(vb[c]) / 450.0, cimag(vb[c]) / 450.0);
+        }
+        dnew[0][m] = -(ik_mul(kx, st[1][m]) + ik_mul(ky, st[2][m]) + ik_mul(kz, st[3][m]));
+        dnew[1][m] = -(ik_mul(kx, Fk[0][m]) + ik_mul(ky, Fk[1][m]) + ik_mul(kz, Fk[2][m])) - v3[0];
+        dnew[2][m] = -(ik_mul(kx, Fk[3][m]) + ik_mul(ky, Fk[4][m]) + ik_mul(kz, Fk[5][m])) - v3[1];
+        dnew[3][m] = -(ik_mul(kx, Fk[6][m]) + ik_mul(ky, Fk[7][m]) + ik_mul(kz, Fk[8][m])) - v3[2];
+        dnew[4][m] = -(ik_mul(kx, Fk[9][m]) + ik_mul(ky, Fk[10][m]) + ik_mul(kz, Fk[11][m])) + rmul(mu, Fk[12][m]);
+        dnew[5][m] = (ik_mul(ky, Fk[13][m]) + ik_mul(kz, Fk[14][m])) - vb[0];
+        dnew[6][m] = -(ik_mul(kx, Fk[15][m]) - ik_mul(kz, Fk[16][m])) - vb[1];
+        dnew[7][m] = -(ik_mul(kx, Fk[17][m]) + ik_mul(ky, Fk[18][m])) - vb[2];
+      }
+  fftw_free(tmp);
+  for (int q = 0; q < 8; q++) fftw_free(R[q]);
+  for (int q = 0; q < 3; q++) { fftw_free(U[q]); fftw_free(uk[q]); }
+  for (int q = 0; q < 9; q++) fftw_free(Dv[q]);
+  for (int q = 0; q < 19; q++) { fftw_free(F[q]); fftw_free(Fk[q]); }
+}
+
+/* ab3com: src/ab3com.f95:44-61 (E_k_new = E_k: its update is commented out) */
+void ora_ab3com(int Nx, int Ny, int Nz, double dt, const ocplx *const st[8], ocplx *const st_new[8],
+                const ocplx *const d_old[8], const ocplx *const d_new[8]) {
+  const size_t nc = (size_t)(Nx / 2 + 1) * Ny * Nz;
+  for (int f = 0; f < 8; f++) {
+    OMP_FOR
+    for (size_t m = 0; m < nc; m++)
+      st_new[f][m] = f == 4 ? st[f][m] : st[f][m] + rmul(dt, rmul(3.0 / 2.0, d_new[f][m]) - rmul(1.0 / 2.0, d_old[f][m]));
+  }
+}
+
+/* time loop of src/main3com.f95:536-600: derive3com, ab3com, d_old = d_new */
+void ora_run3com(int Nx, int Ny, int Nz, double pi, const ora_com3_params *P, int nsteps, ocplx *const st[8],
+                 ocplx *const d_old[8]) {
+  const size_t nc = (size_t)(Nx / 2 + 1) * Ny * Nz;
+  ocplx *dn[8], *sn[8];
+  for (int f = 0; f < 8; f++) { dn[f] = (ocplx *)xmalloc(sizeof(ocplx) * nc); sn[f] = (ocplx *)xmalloc(sizeof(ocplx) * nc); }
+  for (int t = 0; t < nsteps; t++) {
+    ora_derive3com(Nx, Ny, Nz, pi, P, (const ocplx *const *)st, dn);
+    ora_ab3com(Nx, Ny, Nz, P->dt, (const ocplx *const *)st, sn, (const ocplx *const *)d_old, (const ocplx *const *)dn);
+    for (int f = 0; f < 8; f++) {
+      memcpy(d_old[f], dn[f], nc * sizeof(ocplx));
+      memcpy(st[f], sn[f], nc * sizeof(ocplx));
+    }
+  }
+  for (int f = 0; f < 8; f++) { fftw_free(dn[f]); fftw_free(sn[f]); }
+}

@@ -3,7 +3,8 @@
  * TEST INFRASTRUCTURE ONLY.  This is a C restatement of the reference's
  * Fortran subroutines (src/derive2coh.f95, src/ab2coh.f95, src/euler2coh.f95,
  * src/pc*2coh.f95, src/rk4*2coh.f95, src/derive2com.f95, src/ab2com.f95,
- * src/derive2csh.f95, src/ab2csh.f95, src/derive2css.f95, src/ab2css.f95),
+ * src/derive2csh.f95, src/ab2csh.f95, src/derive2css.f95, src/ab2css.f95,
+ * src/derive3com.f95, src/ab3com.f95),
  * linked against the reference's own vendored FFTW 3.3.9 compiled from its
  * sources (oracle/_ref/libfftw3_ref.a).  Only the tests, the smoke check and
  * the CPU-baseline leg of the benchmark may load it, and only as the checker.
@@ -127,6 +128,18 @@ void ora_spectrum_coh(int Nx, int Ny, double pi, const ora_coh_params *P, const 
                       int nbins, double *Ek);
 void ora_spectrum_com(int Nx, int Ny, double pi, const ora_com_params *P, const ocplx *const state[6], int nbins,
                       double *Ek);
+
+/* ---- 3D MHD (src/derive3com.f95, src/ab3com.f95, time loop src/main3com.f95:536-600) ----
+ * arrays: real (Nx,Ny,Nz) a[i + Nx*(j + Ny*k)], complex (Nh,Ny,Nz) a[i + Nh*(j + Ny*k)];
+ * fields rho, rho ux, rho uy, rho uz, E, Bx, By, Bz.  Lx, Ly, Lz as the driver
+ * holds them (already times pi); mu, CS, eta, dt of COMMON /comm/ (src/main3com.f95:56). */
+typedef struct { double Lx, Ly, Lz, mu, CS, eta, dt; } ora_com3_params;
+void ora_derive3com(int Nx, int Ny, int Nz, double pi, const ora_com3_params *P, const ocplx *const st[8],
+                    ocplx *const dnew[8]);
+void ora_ab3com(int Nx, int Ny, int Nz, double dt, const ocplx *const st[8], ocplx *const st_new[8],
+                const ocplx *const d_old[8], const ocplx *const d_new[8]);
+void ora_run3com(int Nx, int Ny, int Nz, double pi, const ora_com3_params *P, int nsteps, ocplx *const st[8],
+                 ocplx *const d_old[8]);
 
 /* number of OpenMP threads the pointwise loops use (0 = runtime default) */
 void ora_set_threads(int n);

@@ -138,6 +138,14 @@ def lib():
         L.tara_ens_num_shells.argtypes = [P, I]
         L.tara_ens_diagnostics.argtypes = [P, I, P, I, P, I]
         L.tara_ens_size.argtypes = [P]
+        L.tara3d_open.argtypes = [C.POINTER(C.c_void_p), I, I, I, C.POINTER(Params3D)]
+        L.tara3d_close.argtypes = [P]
+        L.tara3d_set_params.argtypes = [P, C.POINTER(Params3D)]
+        for n in ("tara3d_set_state", "tara3d_get_state", "tara3d_set_history", "tara3d_rhs"):
+            getattr(L, n).argtypes = [P, PP]
+        L.tara3d_step.argtypes = [P, I]
+        L.tara3d_time_steps.argtypes = [P, I, C.POINTER(C.c_float)]
+        L.tara3d_launches_per_step.argtypes = [P]
         L.tara_num_shells.argtypes = [P]
         L.tara_diagnostics.argtypes = [P, P, I, P, I]
         L.tara_run_recorded.argtypes = [P, I, I, I, P]
@@ -157,6 +165,104 @@ def check(status: int, what: str = "") -> None:
 
 def _ptrs(arrs):
     return (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+
+
+class Params3D(C.Structure):
+    """tara3d_params: pi, box lengths (already times pi), and mu, CS, eta, dt of
+    the 3D driver's COMMON /comm/ (src/main3com.f95:56)."""
+    _fields_ = [(n, C.c_double) for n in ("pi", "Lx", "Ly", "Lz", "mu", "CS", "eta", "dt")] + \
+               [("reserved", C.c_double * 8)]
+
+    @classmethod
+    def make(cls, **kw):
+        p = cls()
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+
+class Mhd3:
+    """3D compressible MHD (src/derive3com.f95, src/ab3com.f95) with the state in
+    HBM.  Fields: rho, rho ux, rho uy, rho uz, E, Bx, By, Bz, each a complex
+    (Nz, Ny, Nx/2+1) array (the reference's Fortran (Nh,Ny,Nz) layout)."""
+
+    NF = 8
+
+    def __init__(self, Nx: int, Ny: int, Nz: int, params: Params3D):
+        self.Nx, self.Ny, self.Nz = Nx, Ny, Nz
+        self.Nh = Nx // 2 + 1
+        self.params = params
+        h = C.c_void_p()
+        check(lib().tara3d_open(C.byref(h), Nx, Ny, Nz, C.byref(params)), "tara3d_open")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().tara3d_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _shape(self):
+        return (self.Nz, self.Ny, self.Nh)
+
+    def _in(self, fields):
+        if len(fields) != self.NF:
+            raise ValueError("8 fields expected")
+        arrs = [np.ascontiguousarray(f, dtype=np.complex128) for f in fields]
+        for a in arrs:
+            if a.shape != self._shape():
+                raise ValueError(f"field shape {a.shape}, expected {self._shape()}")
+        return arrs, (C.c_void_p * self.NF)(*[a.ctypes.data for a in arrs])
+
+    def _out(self):
+        arrs = [np.empty(self._shape(), dtype=np.complex128) for _ in range(self.NF)]
+        return arrs, (C.c_void_p * self.NF)(*[a.ctypes.data for a in arrs])
+
+    def set_params(self, params: Params3D) -> None:
+        check(lib().tara3d_set_params(self._h, C.byref(params)), "tara3d_set_params")
+        self.params = params
+
+    def set_state(self, fields) -> None:
+        arrs, ptrs = self._in(fields)
+        check(lib().tara3d_set_state(self._h, ptrs), "tara3d_set_state")
+
+    def set_history(self, fields) -> None:
+        arrs, ptrs = self._in(fields)
+        check(lib().tara3d_set_history(self._h, ptrs), "tara3d_set_history")
+
+    def get_state(self):
+        arrs, ptrs = self._out()
+        check(lib().tara3d_get_state(self._h, ptrs), "tara3d_get_state")
+        return arrs
+
+    def rhs(self):
+        """derive3com of the current state (d/dt of the 8 fields)."""
+        arrs, ptrs = self._out()
+        check(lib().tara3d_rhs(self._h, ptrs), "tara3d_rhs")
+        return arrs
+
+    def step(self, nsteps: int = 1) -> None:
+        """nsteps of derive3com + ab3com + history shift (src/main3com.f95:548-600)."""
+        check(lib().tara3d_step(self._h, nsteps), "tara3d_step")
+
+    def time_steps(self, nsteps: int) -> float:
+        ms = C.c_float()
+        check(lib().tara3d_time_steps(self._h, nsteps, C.byref(ms)), "tara3d_time_steps")
+        return ms.value
+
+    def launches_per_step(self) -> int:
+        return lib().tara3d_launches_per_step(self._h)
 
 
 class Session:

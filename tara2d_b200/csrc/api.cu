@@ -673,6 +673,11 @@ std::map<std::tuple<int, int, int>, std::unique_ptr<tara_session>> g_legacy;
 
 }  // namespace
 
+namespace tara {
+// status word of the drop-in entry points (tara_legacy_status)
+void set_legacy_status(int s) { g_legacy_status = s; }
+}  // namespace tara
+
 // ======================================================================
 // session API
 // ======================================================================

@@ -1,0 +1,783 @@
+// 3D compressible MHD on the device, FP64: the RHS of src/derive3com.f95:5-1047
+// and the AB2 step of src/ab3com.f95:6-66.
+//
+// Layout: spectral fields [Nz][Ny][Nh] Cx<double>, unpadded (the reference's
+// Fortran (Nh,Ny,Nz) complex(8) arrays, so host buffers copy as they are);
+// real fields [Nz][Ny][Nx] double.
+//
+// 3D c2r (FFTW's rank-3 c2r): complex inverse DFT along z of every (kx, ky)
+// line, along y of every (kx, z) line, then the real inverse along x of every
+// row (the imaginary parts of the kx = 0 and kx = Nx/2 bins ignored).  3D r2c
+// is the reverse.  The z and y passes are one kernel (k_lines3): CB adjacent
+// lines per CTA, so every global load and store of a tile moves CB * 16
+// contiguous bytes; the x pass is one thread group per row.  Both run the
+// Stockham engine of fft_core.cuh.
+//
+// One RHS (derive3com):
+//   state c2r       8 fields, normalised by Nx Ny Nz             (:78-135, :160-177)
+//   k3_velocity     u = (rho u)/rho                                  (:179-182)
+//   velocity r2c    3 fields                                         (:198-215)
+//   derivative c2r  9 fields; i kx / i ky / i kz applied as the z pass loads
+//                   its lines                                       (:244-340)
+//   k3_fluxes       the reference's 19 flux arrays, of which 15 differ: as
+//                   written, Mom_y_1 = Mom_x_2, Mag_y_1 = Mag_x_1,
+//                   Mag_z_1 = Mag_x_2 and Mag_z_2 = Mag_y_2     (:347-414)
+//   flux r2c        15 fields                                        (:416-500)
+//   k3_assemble     i k multiplies, the k^2 terms, the spherical 2/3 mask and
+//                   the sums (:502-1043); while stepping, also ab3com's update
+//                   and the history shift of src/main3com.f95:572-600.
+// The forcing arrays of :184-188 and their transforms (:217-230) do not enter
+// the result (the forcing terms are commented out at :1028-1033) and are not
+// formed.
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+#include "plan.h"
+#include "kernels.cuh"
+
+using namespace tara;
+
+namespace tara {
+void set_legacy_status(int s);
+}
+
+namespace {
+
+constexpr int NSTATE = 8, NDER = 9, NFLUX = 15, MAXJOB = 16;
+enum : int { M3_NONE = 0, M3_IKX = 1, M3_IKY = 2, M3_IKZ = 3 };
+
+bool len3_ok(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512; }
+
+#define TARA3_DISPATCH(n, FN, ...)        \
+  switch (n) {                            \
+    case 16: FN<16>(__VA_ARGS__); break;  \
+    case 32: FN<32>(__VA_ARGS__); break;  \
+    case 64: FN<64>(__VA_ARGS__); break;  \
+    case 128: FN<128>(__VA_ARGS__); break; \
+    case 256: FN<256>(__VA_ARGS__); break; \
+    case 512: FN<512>(__VA_ARGS__); break; \
+    default: break;                       \
+  }
+
+// ------------------------------------------------------------ z and y passes
+struct Line3Job {
+  const Cx<double>* src;
+  Cx<double>* dst;  // may equal src (each CTA reads its whole tile before it writes)
+  int mul;          // M3_*: multiplier applied as the z pass loads (c2r of a derivative)
+};
+struct Line3Args {
+  Line3Job job[MAXJOB];
+  const Cx<double>* tw;  // e^{-2 pi i m/L}, m < L
+  const double *kx, *ky, *kz;
+  long long es;          // element stride along a line (complex elements)
+  long long ps;          // stride between planes
+  int ncol;              // lines per plane, adjacent (stride 1)
+  int tiles;             // tiles of CB lines per plane
+  int Nh;                // z pass: line c is (kx index c % Nh, ky index c / Nh)
+};
+
+// blockIdx.x: (plane, tile of CB lines), blockIdx.y: job
+template <int L, int CB, int P, int DIR>
+__global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_lines3(const Line3Args a) {
+  using F = FFTB<L, CB, P>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<double>* sm = reinterpret_cast<Cx<double>*>(smraw);
+  const Line3Job jb = a.job[blockIdx.y];
+  const int plane = blockIdx.x / a.tiles;
+  const int c0 = (blockIdx.x - plane * a.tiles) * CB;
+  const size_t base = (size_t)plane * (size_t)a.ps;
+  const int tid = threadIdx.x;
+  Cx<double> v[P];
+  fft_run<F, DIR>(sm, tid, v, TwGlobal<double>{a.tw}, [&](int t, int i) -> Cx<double> {
+    const int c = c0 + t;
+    if (c >= a.ncol) return cx<double>(0, 0);
+    const Cx<double> x = ldg(jb.src + base + (size_t)i * (size_t)a.es + c);
+    switch (jb.mul) {
+      case M3_IKX: return ikmul(__ldg(a.kx + c % a.Nh), x);
+      case M3_IKY: return ikmul(__ldg(a.ky + c / a.Nh), x);
+      case M3_IKZ: return ikmul(__ldg(a.kz + i), x);
+      default: return x;
+    }
+  }, SyncBlock{});
+  fft_emit<F>(tid, v, [&](int t, int i, Cx<double> x) {
+    const int c = c0 + t;
+    if (c < a.ncol) st(jb.dst + base + (size_t)i * (size_t)a.es + c, x);
+  });
+}
+
+template <int L, int DIR>
+void launch_lines3(const Line3Args& a0, int njobs, int nplanes, cudaStream_t st) {
+  constexpr int CB = ColCfg<double, L>::CB, P = ColCfg<double, L>::P;
+  using F = FFTB<L, CB, P>;
+  Line3Args a = a0;
+  a.tiles = (a.ncol + CB - 1) / CB;
+  const size_t smem = (size_t)F::SMEM_ELEMS * sizeof(Cx<double>);
+  auto kern = k_lines3<L, CB, P, DIR>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<dim3((unsigned)(a.tiles * nplanes), (unsigned)njobs), CB * L / P, smem, st>>>(a);
+}
+template <int L> void lines3_inv(const Line3Args& a, int nj, int np, cudaStream_t st) {
+  launch_lines3<L, +1>(a, nj, np, st);
+}
+template <int L> void lines3_fwd(const Line3Args& a, int nj, int np, cudaStream_t st) {
+  launch_lines3<L, -1>(a, nj, np, st);
+}
+
+// ------------------------------------------------------------------ x pass
+struct Row3Args {
+  Tables<double> tb;  // tw_row, tw_real, ld = Nh, nn = Nx Ny Nz
+  const Cx<double>* src[MAXJOB];
+  Cx<double>* dst[MAXJOB];
+  int rb;
+};
+
+// c2r along x of half-real rows (pitch Nh) into real rows (Nx/2 pairs),
+// normalised by Nx Ny Nz
+template <int M, int P>
+__global__ void __launch_bounds__(TARA_ROW_LB(M / P)) k_rows3_c2r(const Row3Args a) {
+  using RF = RowFFT<M, P>;
+  constexpr int NTR = M / P;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const RowThread<NTR, 1> th;
+  const auto sync = th.sync();
+  const Tables<double>& tb = a.tb;
+  Cx<double>* xs = reinterpret_cast<Cx<double>*>(smraw) + (size_t)th.row * RF::SMEM_ELEMS;
+  const size_t y = (size_t)blockIdx.x * a.rb + th.row;
+  const Cx<double>* h = a.src[blockIdx.y] + y * tb.ld;
+  Cx<double>* out = a.dst[blockIdx.y] + y * M;
+  Cx<double> v[P];
+  row_c2r<RF>(xs, th.lane, v, tb, [&](int k) { return ldg(h + k); }, sync);
+  fft_emit<RF>(th.lane, v, [&](int, int n, Cx<double> z) {
+    st(out + n, cx<double>(normalise(z.x, tb), normalise(z.y, tb)));
+  });
+}
+
+// r2c along x of real rows into x-transformed rows (pitch Nh)
+template <int M, int P>
+__global__ void __launch_bounds__(TARA_ROW_LB(M / P)) k_rows3_r2c(const Row3Args a) {
+  using RF = RowFFT<M, P>;
+  constexpr int NTR = M / P;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const RowThread<NTR, 1> th;
+  const auto sync = th.sync();
+  const Tables<double>& tb = a.tb;
+  Cx<double>* xs = reinterpret_cast<Cx<double>*>(smraw) + (size_t)th.row * RF::SMEM_ELEMS;
+  const size_t y = (size_t)blockIdx.x * a.rb + th.row;
+  const Cx<double>* in = a.src[blockIdx.y] + y * M;
+  Cx<double>* xo = a.dst[blockIdx.y] + y * tb.ld;
+  Cx<double> v[P];
+  row_r2c_begin<RF>(th.lane, v, tb, [&](int n) { return ldg(in + n); });
+  row_r2c_finish<RF>(xs, th.lane, NTR, v, tb, [&](int k, Cx<double> X) { st(xo + k, X); }, sync);
+}
+
+template <int Nx>
+void launch_rows3(bool inverse, const Row3Args& a0, int nf, int rows, cudaStream_t st) {
+  constexpr int M = Nx / 2;
+  constexpr int P = RowCfg<M>::P;
+  constexpr int NTR = M / P;
+  Row3Args a = a0;
+  const size_t per_row = (size_t)RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<double>);
+  a.rb = 1;
+  while (a.rb * 2 * NTR <= 128 && rows % (a.rb * 2) == 0 && (a.rb * 2) * per_row <= 96 * 1024) a.rb *= 2;
+  const size_t smem = per_row * a.rb;
+  const dim3 grid((unsigned)(rows / a.rb), (unsigned)nf);
+  if (inverse) {
+    auto kern = k_rows3_c2r<M, P>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<grid, NTR * a.rb, smem, st>>>(a);
+  } else {
+    auto kern = k_rows3_r2c<M, P>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<grid, NTR * a.rb, smem, st>>>(a);
+  }
+}
+
+// ------------------------------------------------------------ point kernels
+struct Vel3Args {
+  const double *rho, *mx, *my, *mz;
+  double *ux, *uy, *uz;
+  size_t n;
+};
+// ux = rho_ux/rho ...                                         (src/derive3com.f95:179-182)
+__global__ void k3_velocity(const Vel3Args a) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < a.n; p += (size_t)gridDim.x * blockDim.x) {
+    const double r = a.rho[p];
+    a.ux[p] = a.mx[p] / r;
+    a.uy[p] = a.my[p] / r;
+    a.uz[p] = a.mz[p] / r;
+  }
+}
+
+struct Flux3Args {
+  const double* s[NSTATE];  // rho, rho ux, rho uy, rho uz, E, Bx, By, Bz (real, normalised)
+  const double* d[NDER];    // dux/dx duy/dy duz/dz dBx/dy dBx/dz dBy/dx dBy/dz dBz/dx dBz/dy
+  double* f[NFLUX];
+  double cs, eta;
+  size_t n;
+};
+// Flux order: 0 Mom_x_1, 1 Mom_x_2 (= Mom_y_1), 2 Mom_x_3, 3 Mom_y_2, 4 Mom_y_3,
+// 5 Mom_z_1, 6 Mom_z_2, 7 Mom_z_3, 8 Energy_x, 9 Energy_y, 10 Energy_z,
+// 11 E_Visc, 12 Mag_x_1 (= Mag_y_1), 13 Mag_x_2 (= Mag_z_1), 14 Mag_y_2 (= Mag_z_2)
+__global__ void k3_fluxes(const Flux3Args a) {
+  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < a.n; p += (size_t)gridDim.x * blockDim.x) {
+    const double rho = a.s[0][p], mx = a.s[1][p], my = a.s[2][p], mz = a.s[3][p];
+    const double E = a.s[4][p], Bx = a.s[5][p], By = a.s[6][p], Bz = a.s[7][p];
+    const double ux = mx / rho, uy = my / rho, uz = mz / rho;  // as k3_velocity: the same values
+    const double B2 = Bx * Bx + By * By + Bz * Bz;
+    const double dux = a.d[0][p], duy = a.d[1][p], duz = a.d[2][p];
+    const double dBx_dy = a.d[3][p], dBx_dz = a.d[4][p], dBy_dx = a.d[5][p];
+    const double dBy_dz = a.d[6][p], dBz_dx = a.d[7][p], dBz_dy = a.d[8][p];
+    // curl as the reference defines it                                 (:370-373)
+    const double cx_ = dBz_dy - dBy_dz, cy_ = dBz_dx - dBx_dz, cz_ = dBy_dx - dBx_dy;
+    const double P = a.cs * a.cs * rho;                                // (:375)
+    const double hB2 = B2 / 2.0;
+    a.f[0][p] = mx * ux + P + hB2 - Bx * Bx;                           // (:380-388)
+    a.f[1][p] = mx * uy - Bx * By;
+    a.f[2][p] = mx * uz - Bx * Bz;
+    a.f[3][p] = my * uy + P + hB2 - By * By;
+    a.f[4][p] = my * uz - By * Bz;
+    a.f[5][p] = mz * ux - Bz * Bx;
+    a.f[6][p] = mz * uy - Bz * By;
+    a.f[7][p] = mz * uz + P + hB2 - Bz * Bz;
+    const double H = E + P + hB2;                                      // (:391-399)
+    a.f[8][p] = H * ux - ux * Bx * Bx - uy * Bx * By - uz * Bx * Bz - a.eta * (By * cz_ + Bz * cy_);
+    a.f[9][p] = H * uy - ux * Bx * By - uy * By * By - uz * By * Bz + a.eta * (Bx * cz_ - Bz * cx_);
+    a.f[10][p] = H * uz - ux * Bz * Bx - uy * Bz * By - uz * Bz * Bz + a.eta * (Bx * cy_ + By * cx_);
+    const double dv = dux + duy + duz;                                 // (:402)
+    a.f[11][p] = dv * dv;
+    a.f[12][p] = ux * By - uy * Bx;                                    // (:405-410)
+    a.f[13][p] = ux * Bz - uz * Bx;
+    a.f[14][p] = uy * Bz - uz * By;
+  }
+}
+
+struct Asm3Args {
+  const Cx<double>* f[NFLUX];  // flux spectra
+  const Cx<double>* u[3];      // ux_k, uy_k, uz_k
+  Cx<double>* s[NSTATE];       // state (read; updated in place while stepping)
+  Cx<double>* h[NSTATE];       // history d_old (read, then replaced by d_new) while stepping
+  Cx<double>* out[NSTATE];     // d_new (RHS only)
+  const double *kx, *ky, *kz;
+  double mu, dt, thr;
+  int Nh, Ny, Nz, step;
+};
+
+__device__ __forceinline__ Cx<double> div450(Cx<double> z) { return cx<double>(z.x / 450.0, z.y / 450.0); }
+
+// u + ((3/2) dn - (1/2) dold) dt, every product and sum rounded as written
+// (src/ab3com.f95:47)
+__device__ __forceinline__ double ab2_rn(double u, double dn, double dold, double dt) {
+  return __dadd_rn(u, __dmul_rn(__dsub_rn(__dmul_rn(1.5, dn), __dmul_rn(0.5, dold)), dt));
+}
+__device__ __forceinline__ Cx<double> ab2_rn(Cx<double> u, Cx<double> dn, Cx<double> dold, double dt) {
+  return cx<double>(ab2_rn(u.x, dn.x, dold.x, dt), ab2_rn(u.y, dn.y, dold.y, dt));
+}
+
+// i k multiplies, k^2 terms, mask and sums    (src/derive3com.f95:502-1043);
+// with a.step, ab3com (src/ab3com.f95:44-61) and the history shift
+__global__ void k3_assemble(const Asm3Args a) {
+  const size_t n = (size_t)a.Nh * a.Ny * a.Nz;
+  for (size_t m = blockIdx.x * (size_t)blockDim.x + threadIdx.x; m < n; m += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(m % a.Nh);
+    const size_t r = m / a.Nh;
+    const int j = (int)(r % a.Ny), k = (int)(r / a.Ny);
+    const double kx = __ldg(a.kx + i), ky = __ldg(a.ky + j), kz = __ldg(a.kz + k);
+    // dsqrt(kx*kx + ky*ky + kz*kz) .ge. (dfloat(Nx+Ny+Nz)/3.0)/3.0, each
+    // product and sum rounded as written                                  (:850)
+    const double k2s = __dadd_rn(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky)), __dmul_rn(kz, kz));
+    const bool masked = __dsqrt_rn(k2s) >= a.thr;
+    Cx<double> d[NSTATE];
+    if (masked) {
+#pragma unroll
+      for (int q = 0; q < NSTATE; q++) d[q] = cx<double>(0, 0);
+    } else {
+      const double kx2 = kx * kx, ky2 = ky * ky, kz2 = kz * kz;
+      auto visc = [&](Cx<double> z) { return div450(rmul(kx2, z) + rmul(ky2, z) + rmul(kz2, z)); };
+      auto F = [&](int q) { return ldg(a.f[q] + m); };
+      const Cx<double> rux = ldg(a.s[1] + m), ruy = ldg(a.s[2] + m), ruz = ldg(a.s[3] + m);
+      d[0] = -(ikmul(kx, rux) + ikmul(ky, ruy) + ikmul(kz, ruz));                       // (:1024)
+      d[1] = -(ikmul(kx, F(0)) + ikmul(ky, F(1)) + ikmul(kz, F(2))) - visc(ldg(a.u[0] + m));
+      d[2] = -(ikmul(kx, F(1)) + ikmul(ky, F(3)) + ikmul(kz, F(4))) - visc(ldg(a.u[1] + m));
+      d[3] = -(ikmul(kx, F(5)) + ikmul(ky, F(6)) + ikmul(kz, F(7))) - visc(ldg(a.u[2] + m));
+      d[4] = -(ikmul(kx, F(8)) + ikmul(ky, F(9)) + ikmul(kz, F(10))) + rmul(a.mu, F(11)); // (:1035-1036)
+      d[5] = (ikmul(ky, F(12)) + ikmul(kz, F(13))) - visc(ldg(a.s[5] + m));              // (:1038-1043)
+      d[6] = -(ikmul(kx, F(12)) - ikmul(kz, F(14))) - visc(ldg(a.s[6] + m));
+      d[7] = -(ikmul(kx, F(13)) + ikmul(ky, F(14))) - visc(ldg(a.s[7] + m));
+    }
+    if (!a.step) {
+#pragma unroll
+      for (int q = 0; q < NSTATE; q++) st(a.out[q] + m, d[q]);
+      continue;
+    }
+    // u_new = u + ((3/2) d_new - (1/2) d_old) dt; E unchanged; d_old = d_new
+#pragma unroll
+    for (int q = 0; q < NSTATE; q++) {
+      const Cx<double> old = ld(a.h[q] + m);
+      if (q != 4) {
+        const Cx<double> u = ld(a.s[q] + m);
+        st(a.s[q] + m, ab2_rn(u, d[q], old, a.dt));
+      }
+      st(a.h[q] + m, d[q]);
+    }
+  }
+}
+
+// ab3com alone (the drop-in entry point): out = u + ((3/2) dn - (1/2) dold) dt, E copied
+struct Ab3Args {
+  const Cx<double>* u[NSTATE];
+  const Cx<double>* dn[NSTATE];
+  const Cx<double>* dold[NSTATE];
+  Cx<double>* out[NSTATE];
+  double dt;
+  size_t n;
+};
+__global__ void k3_ab2(const Ab3Args a) {
+  for (size_t m = blockIdx.x * (size_t)blockDim.x + threadIdx.x; m < a.n; m += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NSTATE; q++) {
+      const Cx<double> u = ldg(a.u[q] + m);
+      st(a.out[q] + m, q == 4 ? u : ab2_rn(u, ldg(a.dn[q] + m), ldg(a.dold[q] + m), a.dt));
+    }
+  }
+}
+
+}  // namespace
+
+// ======================================================================
+// session
+// ======================================================================
+struct tara3d {
+  int Nx = 0, Ny = 0, Nz = 0, Nh = 0;
+  size_t ns = 0, nr = 0;  // spectral / real elements per field
+  tara3d_params p{};
+  cudaStream_t st = nullptr;
+  void* tables = nullptr;
+  Tables<double> tb{};
+  const Cx<double>* twy = nullptr;
+  const Cx<double>* twz = nullptr;
+  const double *kx = nullptr, *ky = nullptr, *kz = nullptr;
+  Cx<double>* spec = nullptr;  // one block: state, history, d_new, flux spectra, velocity spectra
+  double* real = nullptr;      // one block: state, velocity, derivative, flux fields
+  Cx<double>* S[NSTATE]{};
+  Cx<double>* H[NSTATE]{};
+  Cx<double>* D[NSTATE]{};
+  Cx<double>* T[NFLUX]{};
+  Cx<double>* U[3]{};
+  double* R[NSTATE]{};
+  double* V[3]{};
+  double* G[NDER]{};
+  double* Fl[NFLUX]{};
+  int grid_pts = 0;
+  cudaGraphExec_t graph = nullptr;
+
+  // 3D c2r of nf fields (src -> real), through the spectral scratch T
+  int c2r(int nf, const Cx<double>* const* src, const int* mul, double* const* dst) {
+    Line3Args z{};
+    for (int q = 0; q < nf; q++) z.job[q] = Line3Job{src[q], T[q], mul ? mul[q] : M3_NONE};
+    z.tw = twz; z.kx = kx; z.ky = ky; z.kz = kz;
+    z.es = (long long)Ny * Nh; z.ps = 0; z.ncol = Ny * Nh; z.Nh = Nh;
+    TARA3_DISPATCH(Nz, lines3_inv, z, nf, 1, st)
+    Line3Args y{};
+    for (int q = 0; q < nf; q++) y.job[q] = Line3Job{T[q], T[q], M3_NONE};
+    y.tw = twy; y.es = Nh; y.ps = (long long)Ny * Nh; y.ncol = Nh; y.Nh = Nh;
+    TARA3_DISPATCH(Ny, lines3_inv, y, nf, Nz, st)
+    Row3Args x{};
+    x.tb = tb;
+    for (int q = 0; q < nf; q++) { x.src[q] = T[q]; x.dst[q] = reinterpret_cast<Cx<double>*>(dst[q]); }
+    TARA3_DISPATCH(Nx, launch_rows3, true, x, nf, Ny * Nz, st)
+    return TARA_OK;
+  }
+  // 3D r2c of nf real fields into dst (x pass writes dst, y and z in place)
+  int r2c(int nf, const double* const* src, Cx<double>* const* dst) {
+    Row3Args x{};
+    x.tb = tb;
+    for (int q = 0; q < nf; q++) { x.src[q] = reinterpret_cast<const Cx<double>*>(src[q]); x.dst[q] = dst[q]; }
+    TARA3_DISPATCH(Nx, launch_rows3, false, x, nf, Ny * Nz, st)
+    Line3Args y{};
+    for (int q = 0; q < nf; q++) y.job[q] = Line3Job{dst[q], dst[q], M3_NONE};
+    y.tw = twy; y.es = Nh; y.ps = (long long)Ny * Nh; y.ncol = Nh; y.Nh = Nh;
+    TARA3_DISPATCH(Ny, lines3_fwd, y, nf, Nz, st)
+    Line3Args z{};
+    for (int q = 0; q < nf; q++) z.job[q] = Line3Job{dst[q], dst[q], M3_NONE};
+    z.tw = twz; z.es = (long long)Ny * Nh; z.ps = 0; z.ncol = Ny * Nh; z.Nh = Nh;
+    TARA3_DISPATCH(Nz, lines3_fwd, z, nf, 1, st)
+    return TARA_OK;
+  }
+
+  // One RHS; step = 0: d_new into D, step = 1: AB2 update of S and H.
+  int rhs(int step) {
+    const Cx<double>* s8[NSTATE];
+    for (int q = 0; q < NSTATE; q++) s8[q] = S[q];
+    TARA_TRY(c2r(NSTATE, s8, nullptr, R));
+    Vel3Args va{R[0], R[1], R[2], R[3], V[0], V[1], V[2], nr};
+    k3_velocity<<<grid_pts, 256, 0, st>>>(va);
+    const double* v3[3] = {V[0], V[1], V[2]};
+    TARA_TRY(r2c(3, v3, U));
+    // i kx ux, i ky uy, i kz uz, i ky Bx, i kz Bx, i kx By, i kz By, i kx Bz, i ky Bz   (:232-340)
+    const Cx<double>* dsrc[NDER] = {U[0], U[1], U[2], S[5], S[5], S[6], S[6], S[7], S[7]};
+    const int dmul[NDER] = {M3_IKX, M3_IKY, M3_IKZ, M3_IKY, M3_IKZ, M3_IKX, M3_IKZ, M3_IKX, M3_IKY};
+    TARA_TRY(c2r(NDER, dsrc, dmul, G));
+    Flux3Args fa{};
+    for (int q = 0; q < NSTATE; q++) fa.s[q] = R[q];
+    for (int q = 0; q < NDER; q++) fa.d[q] = G[q];
+    for (int q = 0; q < NFLUX; q++) fa.f[q] = Fl[q];
+    fa.cs = p.CS; fa.eta = p.eta; fa.n = nr;
+    k3_fluxes<<<grid_pts, 256, 0, st>>>(fa);
+    const double* f15[NFLUX];
+    for (int q = 0; q < NFLUX; q++) f15[q] = Fl[q];
+    TARA_TRY(r2c(NFLUX, f15, T));
+    Asm3Args aa{};
+    for (int q = 0; q < NFLUX; q++) aa.f[q] = T[q];
+    for (int q = 0; q < 3; q++) aa.u[q] = U[q];
+    for (int q = 0; q < NSTATE; q++) { aa.s[q] = S[q]; aa.h[q] = H[q]; aa.out[q] = D[q]; }
+    aa.kx = kx; aa.ky = ky; aa.kz = kz;
+    aa.mu = p.mu; aa.dt = p.dt;
+    aa.thr = ((double)(Nx + Ny + Nz) / 3.0) / 3.0 + 0;
+    aa.Nh = Nh; aa.Ny = Ny; aa.Nz = Nz; aa.step = step;
+    k3_assemble<<<grid_pts, 256, 0, st>>>(aa);
+    TARA_CUDA_TRY(cudaGetLastError());
+    return TARA_OK;
+  }
+
+  int launches_per_step() const { return 3 + 1 + 3 + 3 + 1 + 3 + 1; }
+
+  int steps(int n) {
+    if (n <= 0) return TARA_OK;
+    if (!graph) {
+      // eager first step (sets kernel attributes), then capture one step
+      TARA_TRY(rhs(1));
+      n--;
+      cudaGraph_t g = nullptr;
+      TARA_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const int r = rhs(1);
+      const cudaError_t e = cudaStreamEndCapture(st, &g);
+      if (r != TARA_OK) { if (g) cudaGraphDestroy(g); return r; }
+      TARA_CUDA_TRY(e);
+      const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+      cudaGraphDestroy(g);
+      TARA_CUDA_TRY(ie);
+    }
+    for (int k = 0; k < n; k++) TARA_CUDA_TRY(cudaGraphLaunch(graph, st));
+    TARA_CUDA_TRY(cudaGetLastError());
+    return TARA_OK;
+  }
+
+  int init(int nx, int ny, int nz, const tara3d_params& prm) {
+    if (!len3_ok(nx) || !len3_ok(ny) || !len3_ok(nz)) {
+      set_error("3D grid sizes must be 16, 32, 64, 128, 256 or 512");
+      return TARA_EUNSUPPORTED;
+    }
+    Nx = nx; Ny = ny; Nz = nz; Nh = nx / 2 + 1;
+    ns = (size_t)Nh * Ny * Nz;
+    nr = (size_t)Nx * Ny * Nz;
+    p = prm;
+    TARA_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    int dev = 0, sms = 148;
+    TARA_CUDA_TRY(cudaGetDevice(&dev));
+    TARA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    grid_pts = sms * 8;
+    TARA_TRY(make_tables(sms));
+    // spectral: S, H, D (8 each), T (15), U (3); real: R (8), V (3), G (9), Fl (15)
+    const size_t nspec = 3 * NSTATE + NFLUX + 3, nreal = NSTATE + 3 + NDER + NFLUX;
+    if (cudaMalloc(&spec, nspec * ns * sizeof(Cx<double>)) != cudaSuccess) {
+      spec = nullptr;
+      set_error("cudaMalloc of the 3D spectral fields failed");
+      return TARA_ENOMEM;
+    }
+    if (cudaMalloc(&real, nreal * nr * sizeof(double)) != cudaSuccess) {
+      real = nullptr;
+      set_error("cudaMalloc of the 3D real fields failed");
+      return TARA_ENOMEM;
+    }
+    Cx<double>* c = spec;
+    for (int q = 0; q < NSTATE; q++, c += ns) S[q] = c;
+    for (int q = 0; q < NSTATE; q++, c += ns) H[q] = c;
+    for (int q = 0; q < NSTATE; q++, c += ns) D[q] = c;
+    for (int q = 0; q < NFLUX; q++, c += ns) T[q] = c;
+    for (int q = 0; q < 3; q++, c += ns) U[q] = c;
+    double* r = real;
+    for (int q = 0; q < NSTATE; q++, r += nr) R[q] = r;
+    for (int q = 0; q < 3; q++, r += nr) V[q] = r;
+    for (int q = 0; q < NDER; q++, r += nr) G[q] = r;
+    for (int q = 0; q < NFLUX; q++, r += nr) Fl[q] = r;
+    TARA_CUDA_TRY(cudaMemsetAsync(spec, 0, nspec * ns * sizeof(Cx<double>), st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+
+  int make_tables(int sms) {
+    const int M = Nx / 2;
+    auto tw = [](int L, int count, std::vector<Cx<double>>& out) {
+      out.resize(count);
+      for (int m = 0; m < count; m++) {
+        long double c, s;
+        twiddle(m, L, c, s);
+        out[m] = cx<double>((double)c, (double)s);
+      }
+    };
+    std::vector<Cx<double>> ty, tz, tr, tre;
+    tw(Ny, Ny, ty);
+    tw(Nz, Nz, tz);
+    tw(M, M, tr);
+    tw(Nx, M + 1, tre);
+    // kx = 2.0d0*pi*dfloat(i-1)/Lx; ky, kz negative above N/2   (src/derive3com.f95:237-246)
+    std::vector<double> vkx(Nh), vky(Ny), vkz(Nz);
+    for (int i = 0; i < Nh; i++) vkx[i] = 2.0 * p.pi * (double)i / p.Lx;
+    for (int j = 0; j < Ny; j++) vky[j] = 2.0 * p.pi * (double)(j < Ny / 2 ? j : j - Ny) / p.Ly;
+    for (int k = 0; k < Nz; k++) vkz[k] = 2.0 * p.pi * (double)(k < Nz / 2 ? k : k - Nz) / p.Lz;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t o_ty = 0, o_tz = o_ty + al(ty.size() * 16), o_tr = o_tz + al(tz.size() * 16),
+                 o_tre = o_tr + al(tr.size() * 16), o_kx = o_tre + al(tre.size() * 16),
+                 o_ky = o_kx + al(vkx.size() * 8), o_kz = o_ky + al(vky.size() * 8),
+                 o_status = o_kz + al(vkz.size() * 8), total = o_status + 256;
+    std::vector<char> h(total, 0);
+    std::memcpy(h.data() + o_ty, ty.data(), ty.size() * 16);
+    std::memcpy(h.data() + o_tz, tz.data(), tz.size() * 16);
+    std::memcpy(h.data() + o_tr, tr.data(), tr.size() * 16);
+    std::memcpy(h.data() + o_tre, tre.data(), tre.size() * 16);
+    std::memcpy(h.data() + o_kx, vkx.data(), vkx.size() * 8);
+    std::memcpy(h.data() + o_ky, vky.data(), vky.size() * 8);
+    std::memcpy(h.data() + o_kz, vkz.data(), vkz.size() * 8);
+    if (cudaMalloc(&tables, total) != cudaSuccess) {
+      tables = nullptr;
+      set_error("cudaMalloc of the 3D tables failed");
+      return TARA_ENOMEM;
+    }
+    TARA_CUDA_TRY(cudaMemcpy(tables, h.data(), total, cudaMemcpyHostToDevice));
+    char* b = (char*)tables;
+    twy = (const Cx<double>*)(b + o_ty);
+    twz = (const Cx<double>*)(b + o_tz);
+    kx = (const double*)(b + o_kx);
+    ky = (const double*)(b + o_ky);
+    kz = (const double*)(b + o_kz);
+    tb = Tables<double>{};
+    tb.tw_col = twy;
+    tb.tw_row = (const Cx<double>*)(b + o_tr);
+    tb.tw_real = (const Cx<double>*)(b + o_tre);
+    tb.kx = kx;
+    tb.ky = ky;
+    tb.cut = nullptr;
+    tb.Nx = Nx; tb.Ny = Ny * Nz; tb.Nh = Nh; tb.ld = Nh;
+    const double nn = (double)Nx * (double)Ny * (double)Nz;  // dfloat(Nx)*dfloat(Ny)*dfloat(Nz)
+    tb.nn = nn;
+    tb.inv_nn = 1.0 / nn;
+    tb.nn_pow2 = 1;  // every supported size is a power of two
+    tb.status = (int*)(b + o_status);
+    tb.sm_count = sms;
+    return TARA_OK;
+  }
+
+  void release() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    if (st) cudaStreamSynchronize(st);
+    if (spec) cudaFree(spec);
+    if (real) cudaFree(real);
+    if (tables) cudaFree(tables);
+    if (st) cudaStreamDestroy(st);
+    spec = nullptr; real = nullptr; tables = nullptr; st = nullptr;
+  }
+
+  int upload(Cx<double>* const* dst, const double* const* src) {
+    for (int q = 0; q < NSTATE; q++) {
+      if (!src[q]) { set_error("null field pointer"); return TARA_EINVAL; }
+      TARA_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], ns * sizeof(Cx<double>), cudaMemcpyHostToDevice, st));
+    }
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+  int download(double* const* dst, Cx<double>* const* src) {
+    for (int q = 0; q < NSTATE; q++) {
+      if (!dst[q]) { set_error("null field pointer"); return TARA_EINVAL; }
+      TARA_CUDA_TRY(cudaMemcpyAsync(dst[q], src[q], ns * sizeof(Cx<double>), cudaMemcpyDeviceToHost, st));
+    }
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    return TARA_OK;
+  }
+};
+
+namespace {
+
+bool params_ok(const tara3d_params* p) {
+  if (!p) { set_error("null parameters"); return false; }
+  if (!(p->Lx > 0 && p->Ly > 0 && p->Lz > 0)) { set_error("box lengths must be positive"); return false; }
+  return true;
+}
+
+std::mutex g3_mu;
+std::unique_ptr<tara3d> g3_legacy;  // cached session of the drop-in entry points
+
+tara3d_params params_from_comm(double pi) {
+  // COMMON /comm/ iret,thread_num,time_max,Lx,Ly,Lz,dx,dy,dz,spheat,mu,ms,CS,
+  //               mu_0,eta,dt,kf                               (src/main3com.f95:56)
+  tara3d_params p{};
+  p.pi = pi;
+  p.Lx = comm_[2]; p.Ly = comm_[3]; p.Lz = comm_[4];
+  p.mu = comm_[9]; p.CS = comm_[11]; p.eta = comm_[13]; p.dt = comm_[14];
+  return p;
+}
+
+// Caller holds g3_mu.
+tara3d* legacy3(int Nx, int Ny, int Nz, int Nh, const tara3d_params& p, int& status) {
+  if (Nh != Nx / 2 + 1) { set_error("inconsistent Nx/Nh"); status = TARA_EINVAL; return nullptr; }
+  tara3d* s = g3_legacy.get();
+  const bool same = s && s->Nx == Nx && s->Ny == Ny && s->Nz == Nz && s->p.pi == p.pi && s->p.Lx == p.Lx &&
+                    s->p.Ly == p.Ly && s->p.Lz == p.Lz;
+  if (!same) {
+    if (s) s->release();
+    g3_legacy.reset(new tara3d());
+    s = g3_legacy.get();
+    status = s->init(Nx, Ny, Nz, p);
+    if (status != TARA_OK) { s->release(); g3_legacy.reset(); return nullptr; }
+  }
+  s->p = p;
+  if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }  // parameters are baked into a graph
+  status = TARA_OK;
+  return s;
+}
+
+}  // namespace
+
+// ======================================================================
+// C ABI
+// ======================================================================
+extern "C" {
+
+int tara3d_open(tara3d** out, int Nx, int Ny, int Nz, const tara3d_params* p) {
+  if (!out || !params_ok(p)) { if (!out) set_error("null argument"); return TARA_EINVAL; }
+  *out = nullptr;
+  auto s = std::make_unique<tara3d>();
+  const int r = s->init(Nx, Ny, Nz, *p);
+  if (r != TARA_OK) { s->release(); return r; }
+  *out = s.release();
+  return TARA_OK;
+}
+
+int tara3d_close(tara3d* s) {
+  if (!s) return TARA_EINVAL;
+  s->release();
+  delete s;
+  return TARA_OK;
+}
+
+int tara3d_set_params(tara3d* s, const tara3d_params* p) {
+  if (!s || !params_ok(p)) return TARA_EINVAL;
+  if (p->pi != s->p.pi || p->Lx != s->p.Lx || p->Ly != s->p.Ly || p->Lz != s->p.Lz) {
+    set_error("pi and the box lengths are fixed when the session opens");
+    return TARA_EINVAL;
+  }
+  s->p = *p;
+  if (s->graph) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
+  return TARA_OK;
+}
+
+int tara3d_set_state(tara3d* s, const double* const fields[8]) {
+  if (!s || !fields) { set_error("null argument"); return TARA_EINVAL; }
+  return s->upload(s->S, fields);
+}
+int tara3d_get_state(tara3d* s, double* const fields[8]) {
+  if (!s || !fields) { set_error("null argument"); return TARA_EINVAL; }
+  return s->download(fields, s->S);
+}
+int tara3d_set_history(tara3d* s, const double* const d_old[8]) {
+  if (!s || !d_old) { set_error("null argument"); return TARA_EINVAL; }
+  return s->upload(s->H, d_old);
+}
+int tara3d_rhs(tara3d* s, double* const d_new[8]) {
+  if (!s || !d_new) { set_error("null argument"); return TARA_EINVAL; }
+  TARA_TRY(s->rhs(0));
+  return s->download(d_new, s->D);
+}
+int tara3d_step(tara3d* s, int nsteps) {
+  if (!s || nsteps < 0) { set_error("bad argument"); return TARA_EINVAL; }
+  TARA_TRY(s->steps(nsteps));
+  TARA_CUDA_TRY(cudaStreamSynchronize(s->st));
+  return TARA_OK;
+}
+int tara3d_time_steps(tara3d* s, int nsteps, float* ms) {
+  if (!s || nsteps < 1 || !ms) { set_error("bad argument"); return TARA_EINVAL; }
+  TARA_TRY(s->steps(1));  // builds the graph outside the timed region
+  cudaEvent_t e0, e1;
+  TARA_CUDA_TRY(cudaEventCreate(&e0));
+  TARA_CUDA_TRY(cudaEventCreate(&e1));
+  TARA_CUDA_TRY(cudaStreamSynchronize(s->st));
+  TARA_CUDA_TRY(cudaEventRecord(e0, s->st));
+  const int r = s->steps(nsteps);
+  TARA_CUDA_TRY(cudaEventRecord(e1, s->st));
+  TARA_CUDA_TRY(cudaEventSynchronize(e1));
+  TARA_CUDA_TRY(cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return r;
+}
+int tara3d_launches_per_step(tara3d* s) { return s ? s->launches_per_step() : 0; }
+
+void derive3com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nz, const int32_t* Nh,
+                 const double* pi, const double* time, double* rho_k, double* rho_ux_k,
+                 double* rho_uy_k, double* rho_uz_k, double* E_k, double* Bx_k, double* By_k,
+                 double* Bz_k, double* d_rho_k_dt_old, double* d_rho_k_dt_new,
+                 double* d_rho_ux_k_dt_old, double* d_rho_ux_k_dt_new, double* d_rho_uy_k_dt_old,
+                 double* d_rho_uy_k_dt_new, double* d_rho_uz_k_dt_old, double* d_rho_uz_k_dt_new,
+                 double* d_E_k_dt_old, double* d_E_k_dt_new, double* d_Bx_k_dt_old,
+                 double* d_Bx_k_dt_new, double* d_By_k_dt_old, double* d_By_k_dt_new,
+                 double* d_Bz_k_dt_old, double* d_Bz_k_dt_new) {
+  (void)time; (void)d_rho_k_dt_old; (void)d_rho_ux_k_dt_old; (void)d_rho_uy_k_dt_old;
+  (void)d_rho_uz_k_dt_old; (void)d_E_k_dt_old; (void)d_Bx_k_dt_old; (void)d_By_k_dt_old;
+  (void)d_Bz_k_dt_old;
+  if (!Nx || !Ny || !Nz || !Nh || !pi) { set_error("null argument"); set_legacy_status(TARA_EINVAL); return; }
+  std::lock_guard<std::mutex> lk(g3_mu);
+  int st = TARA_OK;
+  tara3d* s = legacy3(*Nx, *Ny, *Nz, *Nh, params_from_comm(*pi), st);
+  if (s) {
+    const double* in[8] = {rho_k, rho_ux_k, rho_uy_k, rho_uz_k, E_k, Bx_k, By_k, Bz_k};
+    double* out[8] = {d_rho_k_dt_new, d_rho_ux_k_dt_new, d_rho_uy_k_dt_new, d_rho_uz_k_dt_new,
+                      d_E_k_dt_new, d_Bx_k_dt_new, d_By_k_dt_new, d_Bz_k_dt_new};
+    st = s->upload(s->S, in);
+    if (st == TARA_OK) st = s->rhs(0);
+    if (st == TARA_OK) st = s->download(out, s->D);
+  }
+  set_legacy_status(st);
+}
+
+void ab3com_(const int32_t* Nx, const int32_t* Ny, const int32_t* Nz, const int32_t* Nh,
+             const double* pi, const double* time, double* rho_k, double* rho_ux_k, double* rho_uy_k,
+             double* rho_uz_k, double* E_k, double* Bx_k, double* By_k, double* Bz_k,
+             double* rho_k_new, double* rho_ux_k_new, double* rho_uy_k_new, double* rho_uz_k_new,
+             double* E_k_new, double* Bx_k_new, double* By_k_new, double* Bz_k_new,
+             double* d_rho_k_dt_old, double* d_rho_k_dt_new, double* d_rho_ux_k_dt_old,
+             double* d_rho_ux_k_dt_new, double* d_rho_uy_k_dt_old, double* d_rho_uy_k_dt_new,
+             double* d_rho_uz_k_dt_old, double* d_rho_uz_k_dt_new, double* d_E_k_dt_old,
+             double* d_E_k_dt_new, double* d_Bx_k_dt_old, double* d_Bx_k_dt_new,
+             double* d_By_k_dt_old, double* d_By_k_dt_new, double* d_Bz_k_dt_old,
+             double* d_Bz_k_dt_new) {
+  (void)time;
+  if (!Nx || !Ny || !Nz || !Nh || !pi) { set_error("null argument"); set_legacy_status(TARA_EINVAL); return; }
+  std::lock_guard<std::mutex> lk(g3_mu);
+  int st = TARA_OK;
+  tara3d* s = legacy3(*Nx, *Ny, *Nz, *Nh, params_from_comm(*pi), st);
+  if (s) {
+    const double* u[8] = {rho_k, rho_ux_k, rho_uy_k, rho_uz_k, E_k, Bx_k, By_k, Bz_k};
+    const double* dn[8] = {d_rho_k_dt_new, d_rho_ux_k_dt_new, d_rho_uy_k_dt_new, d_rho_uz_k_dt_new,
+                           d_E_k_dt_new, d_Bx_k_dt_new, d_By_k_dt_new, d_Bz_k_dt_new};
+    const double* dol[8] = {d_rho_k_dt_old, d_rho_ux_k_dt_old, d_rho_uy_k_dt_old, d_rho_uz_k_dt_old,
+                            d_E_k_dt_old, d_Bx_k_dt_old, d_By_k_dt_old, d_Bz_k_dt_old};
+    double* out[8] = {rho_k_new, rho_ux_k_new, rho_uy_k_new, rho_uz_k_new, E_k_new, Bx_k_new, By_k_new, Bz_k_new};
+    st = s->upload(s->S, u);
+    if (st == TARA_OK) st = s->upload(s->D, dn);
+    if (st == TARA_OK) st = s->upload(s->H, dol);
+    if (st == TARA_OK) {
+      Ab3Args a{};
+      for (int q = 0; q < 8; q++) { a.u[q] = s->S[q]; a.dn[q] = s->D[q]; a.dold[q] = s->H[q]; a.out[q] = s->T[q]; }
+      a.dt = s->p.dt;
+      a.n = s->ns;
+      k3_ab2<<<s->grid_pts, 256, 0, s->st>>>(a);
+      st = cudaGetLastError() == cudaSuccess ? TARA_OK : TARA_ECUDA;
+      if (st != TARA_OK) set_error("ab3com kernel launch failed");
+    }
+    if (st == TARA_OK) st = s->download(out, s->T);
+  }
+  set_legacy_status(st);
+}
+
+}  // extern "C"

@@ -211,3 +211,25 @@ def hashed_state(model, Nx, Ny, kind, seed, k0=4.0, e1=0.5, e2=0.01, kmin=0.0, k
         X, Y = grid(Nx, Ny, Lx, Ly)
         ux, uy, bx, by = ux - np.sin(Y), uy + np.sin(X), bx - np.sin(Y), by + np.sin(2.0 * X)
     return com_state(np.ones((Ny, Nx)), ux, uy, bx, by, CS, spheat)
+
+
+def mhd3_state(Nx, Ny, Nz, seed=0, noise=1e-3):
+    """Seeded 3D MHD state for the 3D path (src/derive3com.f95): smooth fields
+    (rho ~ 1, |u|, |B| ~ 0.1, E ~ 10) plus Gaussian noise of amplitude `noise`
+    on every grid point, as the spectra of rho, rho ux, rho uy, rho uz, E, Bx,
+    By, Bz, each complex (Nz, Ny, Nx/2+1) (the reference's (Nh,Ny,Nz) layout)."""
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid(np.arange(Nz) * 2 * np.pi / Nz, np.arange(Ny) * 2 * np.pi / Ny,
+                          np.arange(Nx) * 2 * np.pi / Nx, indexing="ij", sparse=True)
+    n = lambda: noise * rng.standard_normal((Nz, Ny, Nx))
+    rho = 1 + 0.1 * np.sin(x + 0.3) * np.cos(y) + n()
+    ux = 0.1 * np.sin(z) + 0.05 * np.cos(x + y) + n()
+    uy = 0.1 * np.cos(x) + n()
+    uz = 0.1 * np.sin(y + 2 * x) + n()
+    out = [np.fft.rfftn(rho), np.fft.rfftn(rho * ux), np.fft.rfftn(rho * uy), np.fft.rfftn(rho * uz)]
+    del ux, uy, uz
+    out.append(np.fft.rfftn(10 + 0.1 * np.cos(x) + n()))
+    out.append(np.fft.rfftn(0.1 * np.cos(z) + n()))
+    out.append(np.fft.rfftn(0.1 * np.sin(x + z) + n()))
+    out.append(np.fft.rfftn(0.05 * np.cos(y) + n()))
+    return out

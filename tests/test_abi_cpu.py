@@ -19,7 +19,7 @@ def declared_symbols():
 def test_header_declares_entry_points():
     names = declared_symbols()
     for must in ("derive2coh_", "ab2coh_", "derive2com_", "ab2com_", "rk4_nk2coh_", "pc_uky2coh_",
-                 "tara_open", "tara_step", "comm_"):
+                 "tara_open", "tara_step", "comm_", "derive3com_", "ab3com_", "tara3d_open", "tara3d_step"):
         assert must in names
 
 
