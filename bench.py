@@ -256,15 +256,31 @@ def run_ensemble(args):
 
 
 # ------------------------------------------------------------------ 3D MHD
+def mhd3_unmasked_fraction(N, L=2 * PI, pi=PI):
+    """Share of the N^3 spectral modes (Nh N N) the 2/3 rule of
+    src/derive3com.f95:850 keeps: sqrt(kx^2 + ky^2 + kz^2) < ((3N)/3)/3."""
+    Nh = N // 2 + 1
+    kx = 2.0 * pi * np.arange(Nh) / L
+    m = np.arange(N)
+    ky = 2.0 * pi * np.where(m < N // 2, m, m - N) / L
+    k2 = (kx[None, None, :] * kx[None, None, :] + ky[None, :, None] * ky[None, :, None]) + \
+        ky[:, None, None] * ky[:, None, None]
+    return float(np.count_nonzero(np.sqrt(k2) < ((3 * N) / 3.0) / 3.0)) / (Nh * N * N)
+
+
 def mhd3_bytes_per_step(N):
     """Algorithmic bytes of one 3D AB2 step at N^3 (every field each kernel must
-    read or write once): 224 S + 74 R, S = spectral field (Nh N N complex128),
-    R = real field (N^3 float64).  c2r of 8 fields 40 S + 8 R, velocity 7 R,
-    r2c of 3 fields 15 S + 3 R, c2r of 9 derivative fields 45 S + 9 R, fluxes
-    32 R, r2c of 15 fluxes 75 S + 15 R, assembly + AB2 49 S."""
+    read or write, once): (191 + 33 f) S + 74 R, S = spectral field (Nh N N
+    complex128), R = real field (N^3 float64), f = unmasked share of the modes.
+    c2r of 8 fields 40 S + 8 R, velocity 7 R, r2c of 3 fields 15 S + 3 R, c2r
+    of 9 derivative fields 45 S + 9 R, fluxes 32 R, r2c of 15 fluxes
+    (45 + 15 + 15 f) S + 15 R (the z pass stores unmasked modes only), assembly
+    + AB2 (31 + 18 f) S (state and history read and written, flux and velocity
+    spectra read where unmasked)."""
     S = (N // 2 + 1) * N * N * 16
     R = N ** 3 * 8
-    return 224 * S + 74 * R
+    f = mhd3_unmasked_fraction(N)
+    return int((191 + 33 * f) * S + 74 * R)
 
 
 def run_mhd3d(args):
@@ -313,7 +329,8 @@ def run_mhd3d(args):
            "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": bps * per_s / 1e9, "peak": peak,
                         "unit": "GB/s", "frac": bps * per_s / 1e9 / peak, "bytes_per_step": bps,
                         "traffic": None, "peak_source": peak_kind,
-                        "note": "224 S + 74 R per AB2 step (every field each kernel reads or writes, once)"},
+                        "note": "(191 + 33 f) S + 74 R per AB2 step, f = unmasked share of the modes "
+                                "(every field each kernel reads or writes, once)"},
            "clocks": clocks, "gpu_launches": launches * K}
     if not args.no_cpu_baseline:
         from oracle import pyoracle as O  # the checker, timed as the CPU baseline only

@@ -64,7 +64,6 @@ bool len3_ok(int n) { return n == 16 || n == 32 || n == 64 || n == 128 || n == 2
 struct Line3Job {
   const Cx<double>* src;
   Cx<double>* dst;  // may equal src (each CTA reads its whole tile before it writes)
-  int mul;          // M3_*: multiplier applied as the z pass loads (c2r of a derivative)
 };
 struct Line3Args {
   Line3Job job[MAXJOB];
@@ -75,53 +74,108 @@ struct Line3Args {
   int ncol;              // lines per plane, adjacent (stride 1)
   int tiles;             // tiles of CB lines per plane
   int Nh;                // z pass: line c is (kx index c % Nh, ky index c / Nh)
+  double thr;            // masked z forward pass: the 2/3-rule threshold
+  double dkz;            // 2 pi / Lz (first guess of the cut-off)
 };
 
-// blockIdx.x: (plane, tile of CB lines), blockIdx.y: job
-template <int L, int CB, int P, int DIR>
+// shared memory of k_lines3: the exchange tile, the kz table, then per line a
+// multiplier and a mask cut-off
+template <int L, int CB, int P> constexpr size_t lines3_smem() {
+  return (size_t)FFTB<L, CB, P>::SMEM_ELEMS * sizeof(Cx<double>) + (L + CB) * sizeof(double) + CB * sizeof(int);
+}
+
+// dsqrt(kx*kx + ky*ky + kz*kz) .ge. thr with kxy = kx*kx + ky*ky, each
+// product and sum rounded as written                    (src/derive3com.f95:850)
+__device__ __forceinline__ bool masked3(double kxy, double kz, double thr) {
+  return __dsqrt_rn(__dadd_rn(kxy, __dmul_rn(kz, kz))) >= thr;
+}
+
+// blockIdx.x: (plane, tile of CB lines), blockIdx.y: job.  MUL: i kx / i ky /
+// i kz applied as the z pass loads (c2r of a derivative); MASK: the forward z
+// pass leaves the modes of the 2/3 rule unwritten.
+template <int L, int CB, int P, int DIR, int MUL, bool MASK>
 __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_lines3(const Line3Args a) {
   using F = FFTB<L, CB, P>;
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<double>* sm = reinterpret_cast<Cx<double>*>(smraw);
+  double* kzs = reinterpret_cast<double*>(sm + F::SMEM_ELEMS);  // kz(i), i < L
+  double* kline = kzs + L;                                       // kx or ky of each line
+  int* cut = reinterpret_cast<int*>(kline + CB);                 // first masked |kz| index of each line
   const Line3Job jb = a.job[blockIdx.y];
   const int plane = blockIdx.x / a.tiles;
   const int c0 = (blockIdx.x - plane * a.tiles) * CB;
   const size_t base = (size_t)plane * (size_t)a.ps;
   const int tid = threadIdx.x;
+  if constexpr (MUL == M3_IKZ) {
+    for (int i = tid; i < L; i += CB * L / P) kzs[i] = __ldg(a.kz + i);
+    __syncthreads();
+  }
+  if constexpr (MUL == M3_IKX || MUL == M3_IKY || MASK) {
+    if (tid < CB) {
+      const int c = c0 + tid;
+      double km = 0.0;
+      int ct = L;
+      if (c < a.ncol) {
+        const double kx = __ldg(a.kx + c % a.Nh), ky = __ldg(a.ky + c / a.Nh);
+        km = MUL == M3_IKX ? kx : ky;
+        if constexpr (MASK) {
+          // first m in 0..L/2 with the line's mode at |kz index| m masked (the test
+          // is monotone in m, and kz(-m)^2 == kz(m)^2 bit for bit): a guess from
+          // the threshold, then exact tests up and down
+          const double kxy = __dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky));
+          const double rem = a.thr * a.thr - kxy;
+          int m = rem > 0.0 ? (int)(sqrt(rem) / a.dkz) : 0;
+          m = m < 0 ? 0 : (m > L / 2 + 1 ? L / 2 + 1 : m);
+          while (m <= L / 2 && !masked3(kxy, __ldg(a.kz + m), a.thr)) m++;
+          while (m > 0 && masked3(kxy, __ldg(a.kz + m - 1), a.thr)) m--;
+          ct = m;
+        }
+      }
+      kline[tid] = km;
+      cut[tid] = ct;
+    }
+    __syncthreads();
+  }
   Cx<double> v[P];
   fft_run<F, DIR>(sm, tid, v, TwGlobal<double>{a.tw}, [&](int t, int i) -> Cx<double> {
     const int c = c0 + t;
     if (c >= a.ncol) return cx<double>(0, 0);
     const Cx<double> x = ldg(jb.src + base + (size_t)i * (size_t)a.es + c);
-    switch (jb.mul) {
-      case M3_IKX: return ikmul(__ldg(a.kx + c % a.Nh), x);
-      case M3_IKY: return ikmul(__ldg(a.ky + c / a.Nh), x);
-      case M3_IKZ: return ikmul(__ldg(a.kz + i), x);
-      default: return x;
-    }
+    if constexpr (MUL == M3_IKX || MUL == M3_IKY) return ikmul(kline[t], x);
+    if constexpr (MUL == M3_IKZ) return ikmul(kzs[i], x);
+    return x;
   }, SyncBlock{});
   fft_emit<F>(tid, v, [&](int t, int i, Cx<double> x) {
     const int c = c0 + t;
-    if (c < a.ncol) st(jb.dst + base + (size_t)i * (size_t)a.es + c, x);
+    if (c >= a.ncol) return;
+    if constexpr (MASK) {
+      if ((i <= L / 2 ? i : L - i) >= cut[t]) return;  // masked: never read
+    }
+    st(jb.dst + base + (size_t)i * (size_t)a.es + c, x);
   });
 }
 
-template <int L, int DIR>
+template <int L, int DIR, int MUL, bool MASK>
 void launch_lines3(const Line3Args& a0, int njobs, int nplanes, cudaStream_t st) {
   constexpr int CB = ColCfg<double, L>::CB, P = ColCfg<double, L>::P;
-  using F = FFTB<L, CB, P>;
   Line3Args a = a0;
   a.tiles = (a.ncol + CB - 1) / CB;
-  const size_t smem = (size_t)F::SMEM_ELEMS * sizeof(Cx<double>);
-  auto kern = k_lines3<L, CB, P, DIR>;
+  const size_t smem = lines3_smem<L, CB, P>();
+  auto kern = k_lines3<L, CB, P, DIR, MUL, MASK>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<dim3((unsigned)(a.tiles * nplanes), (unsigned)njobs), CB * L / P, smem, st>>>(a);
 }
-template <int L> void lines3_inv(const Line3Args& a, int nj, int np, cudaStream_t st) {
-  launch_lines3<L, +1>(a, nj, np, st);
+template <int L> void lines3_inv(const Line3Args& a, int nj, int np, cudaStream_t st, int mul) {
+  switch (mul) {
+    case M3_IKX: launch_lines3<L, +1, M3_IKX, false>(a, nj, np, st); break;
+    case M3_IKY: launch_lines3<L, +1, M3_IKY, false>(a, nj, np, st); break;
+    case M3_IKZ: launch_lines3<L, +1, M3_IKZ, false>(a, nj, np, st); break;
+    default: launch_lines3<L, +1, M3_NONE, false>(a, nj, np, st); break;
+  }
 }
-template <int L> void lines3_fwd(const Line3Args& a, int nj, int np, cudaStream_t st) {
-  launch_lines3<L, -1>(a, nj, np, st);
+template <int L> void lines3_fwd(const Line3Args& a, int nj, int np, cudaStream_t st, bool masked) {
+  if (masked) launch_lines3<L, -1, M3_NONE, true>(a, nj, np, st);
+  else launch_lines3<L, -1, M3_NONE, false>(a, nj, np, st);
 }
 
 // ------------------------------------------------------------------ x pass
@@ -371,37 +425,47 @@ struct tara3d {
   int grid_pts = 0;
   cudaGraphExec_t graph = nullptr;
 
-  // 3D c2r of nf fields (src -> real), through the spectral scratch T
+  // 3D c2r of nf fields (src -> real), through the spectral scratch T; mul[q]
+  // multiplies field q as the z pass loads it (one z launch per multiplier)
   int c2r(int nf, const Cx<double>* const* src, const int* mul, double* const* dst) {
-    Line3Args z{};
-    for (int q = 0; q < nf; q++) z.job[q] = Line3Job{src[q], T[q], mul ? mul[q] : M3_NONE};
-    z.tw = twz; z.kx = kx; z.ky = ky; z.kz = kz;
-    z.es = (long long)Ny * Nh; z.ps = 0; z.ncol = Ny * Nh; z.Nh = Nh;
-    TARA3_DISPATCH(Nz, lines3_inv, z, nf, 1, st)
+    for (int m = M3_NONE; m <= M3_IKZ; m++) {
+      Line3Args z{};
+      int nj = 0;
+      for (int q = 0; q < nf; q++)
+        if ((mul ? mul[q] : M3_NONE) == m) z.job[nj++] = Line3Job{src[q], T[q]};
+      if (nj == 0) continue;
+      z.tw = twz; z.kx = kx; z.ky = ky; z.kz = kz;
+      z.es = (long long)Ny * Nh; z.ps = 0; z.ncol = Ny * Nh; z.Nh = Nh;
+      TARA3_DISPATCH(Nz, lines3_inv, z, nj, 1, st, m)
+    }
     Line3Args y{};
-    for (int q = 0; q < nf; q++) y.job[q] = Line3Job{T[q], T[q], M3_NONE};
+    for (int q = 0; q < nf; q++) y.job[q] = Line3Job{T[q], T[q]};
     y.tw = twy; y.es = Nh; y.ps = (long long)Ny * Nh; y.ncol = Nh; y.Nh = Nh;
-    TARA3_DISPATCH(Ny, lines3_inv, y, nf, Nz, st)
+    TARA3_DISPATCH(Ny, lines3_inv, y, nf, Nz, st, M3_NONE)
     Row3Args x{};
     x.tb = tb;
     for (int q = 0; q < nf; q++) { x.src[q] = T[q]; x.dst[q] = reinterpret_cast<Cx<double>*>(dst[q]); }
     TARA3_DISPATCH(Nx, launch_rows3, true, x, nf, Ny * Nz, st)
     return TARA_OK;
   }
-  // 3D r2c of nf real fields into dst (x pass writes dst, y and z in place)
-  int r2c(int nf, const double* const* src, Cx<double>* const* dst) {
+  // 3D r2c of nf real fields into dst (x pass writes dst, y and z in place);
+  // masked: the z pass leaves the modes of the 2/3 rule unwritten
+  int r2c(int nf, const double* const* src, Cx<double>* const* dst, bool masked) {
     Row3Args x{};
     x.tb = tb;
     for (int q = 0; q < nf; q++) { x.src[q] = reinterpret_cast<const Cx<double>*>(src[q]); x.dst[q] = dst[q]; }
     TARA3_DISPATCH(Nx, launch_rows3, false, x, nf, Ny * Nz, st)
     Line3Args y{};
-    for (int q = 0; q < nf; q++) y.job[q] = Line3Job{dst[q], dst[q], M3_NONE};
+    for (int q = 0; q < nf; q++) y.job[q] = Line3Job{dst[q], dst[q]};
     y.tw = twy; y.es = Nh; y.ps = (long long)Ny * Nh; y.ncol = Nh; y.Nh = Nh;
-    TARA3_DISPATCH(Ny, lines3_fwd, y, nf, Nz, st)
+    TARA3_DISPATCH(Ny, lines3_fwd, y, nf, Nz, st, false)
     Line3Args z{};
-    for (int q = 0; q < nf; q++) z.job[q] = Line3Job{dst[q], dst[q], M3_NONE};
-    z.tw = twz; z.es = (long long)Ny * Nh; z.ps = 0; z.ncol = Ny * Nh; z.Nh = Nh;
-    TARA3_DISPATCH(Nz, lines3_fwd, z, nf, 1, st)
+    for (int q = 0; q < nf; q++) z.job[q] = Line3Job{dst[q], dst[q]};
+    z.tw = twz; z.kx = kx; z.ky = ky; z.kz = kz;
+    z.es = (long long)Ny * Nh; z.ps = 0; z.ncol = Ny * Nh; z.Nh = Nh;
+    z.thr = mask_thr();
+    z.dkz = 2.0 * p.pi / p.Lz;
+    TARA3_DISPATCH(Nz, lines3_fwd, z, nf, 1, st, masked)
     return TARA_OK;
   }
 
@@ -413,7 +477,7 @@ struct tara3d {
     Vel3Args va{R[0], R[1], R[2], R[3], V[0], V[1], V[2], nr};
     k3_velocity<<<grid_pts, 256, 0, st>>>(va);
     const double* v3[3] = {V[0], V[1], V[2]};
-    TARA_TRY(r2c(3, v3, U));
+    TARA_TRY(r2c(3, v3, U, false));  // every mode: the derivatives below use them all
     // i kx ux, i ky uy, i kz uz, i ky Bx, i kz Bx, i kx By, i kz By, i kx Bz, i ky Bz   (:232-340)
     const Cx<double>* dsrc[NDER] = {U[0], U[1], U[2], S[5], S[5], S[6], S[6], S[7], S[7]};
     const int dmul[NDER] = {M3_IKX, M3_IKY, M3_IKZ, M3_IKY, M3_IKZ, M3_IKX, M3_IKZ, M3_IKX, M3_IKY};
@@ -426,21 +490,24 @@ struct tara3d {
     k3_fluxes<<<grid_pts, 256, 0, st>>>(fa);
     const double* f15[NFLUX];
     for (int q = 0; q < NFLUX; q++) f15[q] = Fl[q];
-    TARA_TRY(r2c(NFLUX, f15, T));
+    TARA_TRY(r2c(NFLUX, f15, T, true));  // k3_assemble reads unmasked modes only
     Asm3Args aa{};
     for (int q = 0; q < NFLUX; q++) aa.f[q] = T[q];
     for (int q = 0; q < 3; q++) aa.u[q] = U[q];
     for (int q = 0; q < NSTATE; q++) { aa.s[q] = S[q]; aa.h[q] = H[q]; aa.out[q] = D[q]; }
     aa.kx = kx; aa.ky = ky; aa.kz = kz;
     aa.mu = p.mu; aa.dt = p.dt;
-    aa.thr = ((double)(Nx + Ny + Nz) / 3.0) / 3.0 + 0;
+    aa.thr = mask_thr();
     aa.Nh = Nh; aa.Ny = Ny; aa.Nz = Nz; aa.step = step;
     k3_assemble<<<grid_pts, 256, 0, st>>>(aa);
     TARA_CUDA_TRY(cudaGetLastError());
     return TARA_OK;
   }
 
-  int launches_per_step() const { return 3 + 1 + 3 + 3 + 1 + 3 + 1; }
+  // (dfloat(Nx+Ny+Nz)/3.0)/3.0 + 0                                  (src/derive3com.f95:850)
+  double mask_thr() const { return ((double)(Nx + Ny + Nz) / 3.0) / 3.0 + 0; }
+
+  int launches_per_step() const { return 3 + 1 + 3 + 5 + 1 + 3 + 1; }
 
   int steps(int n) {
     if (n <= 0) return TARA_OK;
