@@ -270,17 +270,18 @@ def mhd3_unmasked_fraction(N, L=2 * PI, pi=PI):
 
 def mhd3_bytes_per_step(N):
     """Algorithmic bytes of one 3D AB2 step at N^3 (every field each kernel must
-    read or write, once): (191 + 33 f) S + 74 R, S = spectral field (Nh N N
+    read or write, once): (191 + 33 f) S + 44 R, S = spectral field (Nh N N
     complex128), R = real field (N^3 float64), f = unmasked share of the modes.
     c2r of 8 fields 40 S + 8 R, velocity 7 R, r2c of 3 fields 15 S + 3 R, c2r
-    of 9 derivative fields 45 S + 9 R, fluxes 32 R, r2c of 15 fluxes
-    (45 + 15 + 15 f) S + 15 R (the z pass stores unmasked modes only), assembly
-    + AB2 (31 + 18 f) S (state and history read and written, flux and velocity
-    spectra read where unmasked)."""
+    of 9 derivative fields 45 S + 9 R, fluxes with their x r2c in one row
+    kernel 17 R + 15 S, y and z passes of the 15 flux fields (45 + 15 f) S
+    (the z pass stores unmasked modes only), assembly + AB2 (31 + 18 f) S
+    (state and history read and written, flux and velocity spectra read where
+    unmasked)."""
     S = (N // 2 + 1) * N * N * 16
     R = N ** 3 * 8
     f = mhd3_unmasked_fraction(N)
-    return int((191 + 33 * f) * S + 74 * R)
+    return int((191 + 33 * f) * S + 44 * R)
 
 
 def run_mhd3d(args):
@@ -321,7 +322,7 @@ def run_mhd3d(args):
            "config": {"workload": f"3D compressible MHD (*3com), {N}^3, FP64, AB2 dt=1e-4, mu=0.01, CS=10, "
                                   "eta=0.005, smooth fields + 1e-4 noise (seed 0)",
                       "grid": [N, N, N],
-                      "l2": f"working set {(42 * field + 35 * N ** 3 * 8) / 1e9:.1f} GB > 126 MB L2; no flush"},
+                      "l2": f"working set {(42 * field + 20 * N ** 3 * 8) / 1e9:.1f} GB > 126 MB L2; no flush"},
            "grid_point_steps_per_s": per_s * N ** 3,
            "e2e": {"value": 1.0 / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": 8 * field,
                    "d2h_bytes_per_step": 8 * field,
@@ -329,7 +330,7 @@ def run_mhd3d(args):
            "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": bps * per_s / 1e9, "peak": peak,
                         "unit": "GB/s", "frac": bps * per_s / 1e9 / peak, "bytes_per_step": bps,
                         "traffic": None, "peak_source": peak_kind,
-                        "note": "(191 + 33 f) S + 74 R per AB2 step, f = unmasked share of the modes "
+                        "note": "(191 + 33 f) S + 44 R per AB2 step, f = unmasked share of the modes "
                                 "(every field each kernel reads or writes, once)"},
            "clocks": clocks, "gpu_launches": launches * K}
     if not args.no_cpu_baseline:

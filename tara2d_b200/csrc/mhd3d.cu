@@ -19,10 +19,11 @@
 //   velocity r2c    3 fields                                         (:198-215)
 //   derivative c2r  9 fields; i kx / i ky / i kz applied as the z pass loads
 //                   its lines                                       (:244-340)
-//   k3_fluxes       the reference's 19 flux arrays, of which 15 differ: as
-//                   written, Mom_y_1 = Mom_x_2, Mag_y_1 = Mag_x_1,
-//                   Mag_z_1 = Mag_x_2 and Mag_z_2 = Mag_y_2     (:347-414)
-//   flux r2c        15 fields                                        (:416-500)
+//   k_rows3_flux    per row: the reference's 19 flux arrays, of which 15
+//                   differ (as written, Mom_y_1 = Mom_x_2, Mag_y_1 = Mag_x_1,
+//                   Mag_z_1 = Mag_x_2, Mag_z_2 = Mag_y_2)   (:347-414),
+//                   and their r2c along x, in shared memory        (:416-500)
+//   flux y, z       forward passes of the 15 flux fields
 //   k3_assemble     i k multiplies, the k^2 terms, the spherical 2/3 mask and
 //                   the sums (:502-1043); while stepping, also ab3com's update
 //                   and the history shift of src/main3com.f95:572-600.
@@ -263,47 +264,108 @@ __global__ void k3_velocity(const Vel3Args a) {
   }
 }
 
-struct Flux3Args {
+// The 15 distinct fluxes of one point from its 8 state and 9 derivative
+// values (real space, normalised).  Order: 0 Mom_x_1, 1 Mom_x_2 (= Mom_y_1),
+// 2 Mom_x_3, 3 Mom_y_2, 4 Mom_y_3, 5 Mom_z_1, 6 Mom_z_2, 7 Mom_z_3,
+// 8 Energy_x, 9 Energy_y, 10 Energy_z, 11 E_Visc, 12 Mag_x_1 (= Mag_y_1),
+// 13 Mag_x_2 (= Mag_z_1), 14 Mag_y_2 (= Mag_z_2)
+__device__ __forceinline__ void fluxes15(const double* s, const double* d, double cs, double eta, double* f) {
+  const double rho = s[0], mx = s[1], my = s[2], mz = s[3], E = s[4], Bx = s[5], By = s[6], Bz = s[7];
+  const double ux = mx / rho, uy = my / rho, uz = mz / rho;  // as k3_velocity: the same values
+  const double B2 = Bx * Bx + By * By + Bz * Bz;
+  // curl as the reference defines it                                 (:370-373)
+  const double cx_ = d[8] - d[6], cy_ = d[7] - d[4], cz_ = d[5] - d[3];
+  const double P = cs * cs * rho;                                    // (:375)
+  const double hB2 = B2 / 2.0;
+  f[0] = mx * ux + P + hB2 - Bx * Bx;                                // (:380-388)
+  f[1] = mx * uy - Bx * By;
+  f[2] = mx * uz - Bx * Bz;
+  f[3] = my * uy + P + hB2 - By * By;
+  f[4] = my * uz - By * Bz;
+  f[5] = mz * ux - Bz * Bx;
+  f[6] = mz * uy - Bz * By;
+  f[7] = mz * uz + P + hB2 - Bz * Bz;
+  const double H = E + P + hB2;                                      // (:391-399)
+  f[8] = H * ux - ux * Bx * Bx - uy * Bx * By - uz * Bx * Bz - eta * (By * cz_ + Bz * cy_);
+  f[9] = H * uy - ux * Bx * By - uy * By * By - uz * By * Bz + eta * (Bx * cz_ - Bz * cx_);
+  f[10] = H * uz - ux * Bz * Bx - uy * Bz * By - uz * Bz * Bz + eta * (Bx * cy_ + By * cx_);
+  const double dv = d[0] + d[1] + d[2];                              // (:402)
+  f[11] = dv * dv;
+  f[12] = ux * By - uy * Bx;                                         // (:405-410)
+  f[13] = ux * Bz - uz * Bx;
+  f[14] = uy * Bz - uz * By;
+}
+
+// Fluxes and their r2c along x in one row kernel: per row, every thread of
+// the row forms the 15 fluxes of its point pairs (x[2n], x[2n+1]) into 15
+// shared-memory rows, then 15 thread groups run one r2c each, using their own
+// row as exchange buffer.  The real flux fields never reach HBM.
+struct FluxRowArgs {
+  Tables<double> tb;
   const double* s[NSTATE];  // rho, rho ux, rho uy, rho uz, E, Bx, By, Bz (real, normalised)
   const double* d[NDER];    // dux/dx duy/dy duz/dz dBx/dy dBx/dz dBy/dx dBy/dz dBz/dx dBz/dy
-  double* f[NFLUX];
+  Cx<double>* x[NFLUX];     // x-transformed flux rows (pitch Nh)
   double cs, eta;
-  size_t n;
+  int rb;
 };
-// Flux order: 0 Mom_x_1, 1 Mom_x_2 (= Mom_y_1), 2 Mom_x_3, 3 Mom_y_2, 4 Mom_y_3,
-// 5 Mom_z_1, 6 Mom_z_2, 7 Mom_z_3, 8 Energy_x, 9 Energy_y, 10 Energy_z,
-// 11 E_Visc, 12 Mag_x_1 (= Mag_y_1), 13 Mag_x_2 (= Mag_z_1), 14 Mag_y_2 (= Mag_z_2)
-__global__ void k3_fluxes(const Flux3Args a) {
-  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < a.n; p += (size_t)gridDim.x * blockDim.x) {
-    const double rho = a.s[0][p], mx = a.s[1][p], my = a.s[2][p], mz = a.s[3][p];
-    const double E = a.s[4][p], Bx = a.s[5][p], By = a.s[6][p], Bz = a.s[7][p];
-    const double ux = mx / rho, uy = my / rho, uz = mz / rho;  // as k3_velocity: the same values
-    const double B2 = Bx * Bx + By * By + Bz * Bz;
-    const double dux = a.d[0][p], duy = a.d[1][p], duz = a.d[2][p];
-    const double dBx_dy = a.d[3][p], dBx_dz = a.d[4][p], dBy_dx = a.d[5][p];
-    const double dBy_dz = a.d[6][p], dBz_dx = a.d[7][p], dBz_dy = a.d[8][p];
-    // curl as the reference defines it                                 (:370-373)
-    const double cx_ = dBz_dy - dBy_dz, cy_ = dBz_dx - dBx_dz, cz_ = dBy_dx - dBx_dy;
-    const double P = a.cs * a.cs * rho;                                // (:375)
-    const double hB2 = B2 / 2.0;
-    a.f[0][p] = mx * ux + P + hB2 - Bx * Bx;                           // (:380-388)
-    a.f[1][p] = mx * uy - Bx * By;
-    a.f[2][p] = mx * uz - Bx * Bz;
-    a.f[3][p] = my * uy + P + hB2 - By * By;
-    a.f[4][p] = my * uz - By * Bz;
-    a.f[5][p] = mz * ux - Bz * Bx;
-    a.f[6][p] = mz * uy - Bz * By;
-    a.f[7][p] = mz * uz + P + hB2 - Bz * Bz;
-    const double H = E + P + hB2;                                      // (:391-399)
-    a.f[8][p] = H * ux - ux * Bx * Bx - uy * Bx * By - uz * Bx * Bz - a.eta * (By * cz_ + Bz * cy_);
-    a.f[9][p] = H * uy - ux * Bx * By - uy * By * By - uz * By * Bz + a.eta * (Bx * cz_ - Bz * cx_);
-    a.f[10][p] = H * uz - ux * Bz * Bx - uy * Bz * By - uz * Bz * Bz + a.eta * (Bx * cy_ + By * cx_);
-    const double dv = dux + duy + duz;                                 // (:402)
-    a.f[11][p] = dv * dv;
-    a.f[12][p] = ux * By - uy * Bx;                                    // (:405-410)
-    a.f[13][p] = ux * Bz - uz * Bx;
-    a.f[14][p] = uy * Bz - uz * By;
+template <int M, int P>
+__global__ void __launch_bounds__(TARA_ROW_LB(NFLUX * (M / P))) k_rows3_flux(const FluxRowArgs a) {
+  using RF = RowFFT<M, P>;
+  constexpr int NTR = M / P, G = NFLUX, ARR = RF::SMEM_ELEMS;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const RowThread<NTR, G> th;
+  const auto sync = th.sync();
+  const Tables<double>& tb = a.tb;
+  Cx<double>* base = reinterpret_cast<Cx<double>*>(smraw) + (size_t)th.row * G * ARR;
+  const size_t y = (size_t)blockIdx.x * a.rb + th.row;
+  const size_t ro = y * (size_t)(2 * M);
+  // phase 1: fluxes of the point pairs n (x = 2n, 2n+1)                (:343-414)
+  for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
+    double sv[2][NSTATE], dv[2][NDER];
+#pragma unroll
+    for (int q = 0; q < NSTATE; q++) {
+      const double2 w = __ldg(reinterpret_cast<const double2*>(a.s[q] + ro) + n);
+      sv[0][q] = w.x;
+      sv[1][q] = w.y;
+    }
+#pragma unroll
+    for (int q = 0; q < NDER; q++) {
+      const double2 w = __ldg(reinterpret_cast<const double2*>(a.d[q] + ro) + n);
+      dv[0][q] = w.x;
+      dv[1][q] = w.y;
+    }
+    double f0[NFLUX], f1[NFLUX];
+    fluxes15(sv[0], dv[0], a.cs, a.eta, f0);
+    fluxes15(sv[1], dv[1], a.cs, a.eta, f1);
+#pragma unroll
+    for (int q = 0; q < NFLUX; q++) base[q * ARR + n] = cx<double>(f0[q], f1[q]);
   }
+  __syncthreads();
+  // phase 2: r2c along x of flux g, exchanges in its own row (every value of
+  // the row is in registers before the first exchange store)     (:416-500)
+  Cx<double>* arr = base + th.g * ARR;
+  Cx<double> v[P];
+  row_r2c_begin<RF>(th.lane, v, tb, [&](int n) { return arr[n]; });
+  Cx<double>* xo = a.x[th.g] + y * tb.ld;
+  row_r2c_finish<RF>(arr, th.lane, NTR, v, tb, [&](int k, Cx<double> X) { st(xo + k, X); }, sync);
+}
+
+template <int Nx>
+void launch_rows3_flux(const FluxRowArgs& a0, int rows, cudaStream_t st) {
+  constexpr int M = Nx / 2;
+  constexpr int P = RowCfg<M>::P;
+  constexpr int NTR = M / P;
+  FluxRowArgs a = a0;
+  const size_t per_row = (size_t)NFLUX * RowFFT<M, P>::SMEM_ELEMS * sizeof(Cx<double>);
+  a.rb = 1;
+  // rows per CTA within the kernel's launch bound
+  while ((a.rb * 2) * NFLUX * NTR <= TARA_ROW_LB(NFLUX * NTR) && rows % (a.rb * 2) == 0 &&
+         (a.rb * 2) * per_row <= 100 * 1024)
+    a.rb *= 2;
+  const size_t smem = per_row * a.rb;
+  auto kern = k_rows3_flux<M, P>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<(unsigned)(rows / a.rb), NFLUX * NTR * a.rb, smem, st>>>(a);
 }
 
 struct Asm3Args {
@@ -412,7 +474,7 @@ struct tara3d {
   const Cx<double>* twz = nullptr;
   const double *kx = nullptr, *ky = nullptr, *kz = nullptr;
   Cx<double>* spec = nullptr;  // one block: state, history, d_new, flux spectra, velocity spectra
-  double* real = nullptr;      // one block: state, velocity, derivative, flux fields
+  double* real = nullptr;      // one block: state, velocity and derivative fields
   Cx<double>* S[NSTATE]{};
   Cx<double>* H[NSTATE]{};
   Cx<double>* D[NSTATE]{};
@@ -421,7 +483,6 @@ struct tara3d {
   double* R[NSTATE]{};
   double* V[3]{};
   double* G[NDER]{};
-  double* Fl[NFLUX]{};
   int grid_pts = 0;
   cudaGraphExec_t graph = nullptr;
 
@@ -455,6 +516,10 @@ struct tara3d {
     x.tb = tb;
     for (int q = 0; q < nf; q++) { x.src[q] = reinterpret_cast<const Cx<double>*>(src[q]); x.dst[q] = dst[q]; }
     TARA3_DISPATCH(Nx, launch_rows3, false, x, nf, Ny * Nz, st)
+    return fwd_yz(nf, dst, masked);
+  }
+  // forward y and z passes in place of nf x-transformed fields
+  int fwd_yz(int nf, Cx<double>* const* dst, bool masked) {
     Line3Args y{};
     for (int q = 0; q < nf; q++) y.job[q] = Line3Job{dst[q], dst[q]};
     y.tw = twy; y.es = Nh; y.ps = (long long)Ny * Nh; y.ncol = Nh; y.Nh = Nh;
@@ -482,15 +547,14 @@ struct tara3d {
     const Cx<double>* dsrc[NDER] = {U[0], U[1], U[2], S[5], S[5], S[6], S[6], S[7], S[7]};
     const int dmul[NDER] = {M3_IKX, M3_IKY, M3_IKZ, M3_IKY, M3_IKZ, M3_IKX, M3_IKZ, M3_IKX, M3_IKY};
     TARA_TRY(c2r(NDER, dsrc, dmul, G));
-    Flux3Args fa{};
+    FluxRowArgs fa{};
+    fa.tb = tb;
     for (int q = 0; q < NSTATE; q++) fa.s[q] = R[q];
     for (int q = 0; q < NDER; q++) fa.d[q] = G[q];
-    for (int q = 0; q < NFLUX; q++) fa.f[q] = Fl[q];
-    fa.cs = p.CS; fa.eta = p.eta; fa.n = nr;
-    k3_fluxes<<<grid_pts, 256, 0, st>>>(fa);
-    const double* f15[NFLUX];
-    for (int q = 0; q < NFLUX; q++) f15[q] = Fl[q];
-    TARA_TRY(r2c(NFLUX, f15, T, true));  // k3_assemble reads unmasked modes only
+    for (int q = 0; q < NFLUX; q++) fa.x[q] = T[q];
+    fa.cs = p.CS; fa.eta = p.eta;
+    TARA3_DISPATCH(Nx, launch_rows3_flux, fa, Ny * Nz, st)
+    TARA_TRY(fwd_yz(NFLUX, T, true));  // k3_assemble reads unmasked modes only
     Asm3Args aa{};
     for (int q = 0; q < NFLUX; q++) aa.f[q] = T[q];
     for (int q = 0; q < 3; q++) aa.u[q] = U[q];
@@ -507,7 +571,7 @@ struct tara3d {
   // (dfloat(Nx+Ny+Nz)/3.0)/3.0 + 0                                  (src/derive3com.f95:850)
   double mask_thr() const { return ((double)(Nx + Ny + Nz) / 3.0) / 3.0 + 0; }
 
-  int launches_per_step() const { return 3 + 1 + 3 + 5 + 1 + 3 + 1; }
+  int launches_per_step() const { return 3 + 1 + 3 + 5 + 1 + 2 + 1; }
 
   int steps(int n) {
     if (n <= 0) return TARA_OK;
@@ -545,8 +609,8 @@ struct tara3d {
     TARA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     grid_pts = sms * 8;
     TARA_TRY(make_tables(sms));
-    // spectral: S, H, D (8 each), T (15), U (3); real: R (8), V (3), G (9), Fl (15)
-    const size_t nspec = 3 * NSTATE + NFLUX + 3, nreal = NSTATE + 3 + NDER + NFLUX;
+    // spectral: S, H, D (8 each), T (15), U (3); real: R (8), V (3), G (9)
+    const size_t nspec = 3 * NSTATE + NFLUX + 3, nreal = NSTATE + 3 + NDER;
     if (cudaMalloc(&spec, nspec * ns * sizeof(Cx<double>)) != cudaSuccess) {
       spec = nullptr;
       set_error("cudaMalloc of the 3D spectral fields failed");
@@ -567,7 +631,6 @@ struct tara3d {
     for (int q = 0; q < NSTATE; q++, r += nr) R[q] = r;
     for (int q = 0; q < 3; q++, r += nr) V[q] = r;
     for (int q = 0; q < NDER; q++, r += nr) G[q] = r;
-    for (int q = 0; q < NFLUX; q++, r += nr) Fl[q] = r;
     TARA_CUDA_TRY(cudaMemsetAsync(spec, 0, nspec * ns * sizeof(Cx<double>), st));
     TARA_CUDA_TRY(cudaStreamSynchronize(st));
     return TARA_OK;
