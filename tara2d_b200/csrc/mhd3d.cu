@@ -308,8 +308,11 @@ struct FluxRowArgs {
   double cs, eta;
   int rb;
 };
+// Five CTAs per SM where a CTA has at most 128 threads (92 registers, no
+// spills; 20 instead of 15 warps per SM at Nx = 256)
 template <int M, int P>
-__global__ void __launch_bounds__(TARA_ROW_LB(NFLUX * (M / P))) k_rows3_flux(const FluxRowArgs a) {
+__global__ void __launch_bounds__(TARA_ROW_LB(NFLUX * (M / P)), (NFLUX * (M / P) <= 128 ? 5 : 1))
+    k_rows3_flux(const FluxRowArgs a) {
   using RF = RowFFT<M, P>;
   constexpr int NTR = M / P, G = NFLUX, ARR = RF::SMEM_ELEMS;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -320,25 +323,18 @@ __global__ void __launch_bounds__(TARA_ROW_LB(NFLUX * (M / P))) k_rows3_flux(con
   const size_t y = (size_t)blockIdx.x * a.rb + th.row;
   const size_t ro = y * (size_t)(2 * M);
   // phase 1: fluxes of the point pairs n (x = 2n, 2n+1)                (:343-414)
-  for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
-    double sv[2][NSTATE], dv[2][NDER];
+  // one point at a time (x = 2n + h into component h of the pair), which keeps
+  // few values live
+  double* basd = reinterpret_cast<double*>(base);
+  for (int e = th.g * NTR + th.lane; e < 2 * M; e += G * NTR) {
+    double sv[NSTATE], dv[NDER], f[NFLUX];
 #pragma unroll
-    for (int q = 0; q < NSTATE; q++) {
-      const double2 w = __ldg(reinterpret_cast<const double2*>(a.s[q] + ro) + n);
-      sv[0][q] = w.x;
-      sv[1][q] = w.y;
-    }
+    for (int q = 0; q < NSTATE; q++) sv[q] = __ldg(a.s[q] + ro + e);
 #pragma unroll
-    for (int q = 0; q < NDER; q++) {
-      const double2 w = __ldg(reinterpret_cast<const double2*>(a.d[q] + ro) + n);
-      dv[0][q] = w.x;
-      dv[1][q] = w.y;
-    }
-    double f0[NFLUX], f1[NFLUX];
-    fluxes15(sv[0], dv[0], a.cs, a.eta, f0);
-    fluxes15(sv[1], dv[1], a.cs, a.eta, f1);
+    for (int q = 0; q < NDER; q++) dv[q] = __ldg(a.d[q] + ro + e);
+    fluxes15(sv, dv, a.cs, a.eta, f);
 #pragma unroll
-    for (int q = 0; q < NFLUX; q++) base[q * ARR + n] = cx<double>(f0[q], f1[q]);
+    for (int q = 0; q < NFLUX; q++) basd[2 * q * ARR + e] = f[q];
   }
   __syncthreads();
   // phase 2: r2c along x of flux g, exchanges in its own row (every value of
