@@ -189,8 +189,9 @@ struct Row3Args {
 
 // c2r along x of half-real rows (pitch Nh) into real rows (Nx/2 pairs),
 // normalised by Nx Ny Nz
+// five CTAs per SM (at most 96 registers) in both x-pass kernels
 template <int M, int P>
-__global__ void __launch_bounds__(TARA_ROW_LB(M / P)) k_rows3_c2r(const Row3Args a) {
+__global__ void __launch_bounds__(TARA_ROW_LB(M / P), 5) k_rows3_c2r(const Row3Args a) {
   using RF = RowFFT<M, P>;
   constexpr int NTR = M / P;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -210,7 +211,7 @@ __global__ void __launch_bounds__(TARA_ROW_LB(M / P)) k_rows3_c2r(const Row3Args
 
 // r2c along x of real rows into x-transformed rows (pitch Nh)
 template <int M, int P>
-__global__ void __launch_bounds__(TARA_ROW_LB(M / P)) k_rows3_r2c(const Row3Args a) {
+__global__ void __launch_bounds__(TARA_ROW_LB(M / P), 5) k_rows3_r2c(const Row3Args a) {
   using RF = RowFFT<M, P>;
   constexpr int NTR = M / P;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -388,7 +389,7 @@ __device__ __forceinline__ Cx<double> ab2_rn(Cx<double> u, Cx<double> dn, Cx<dou
 
 // i k multiplies, k^2 terms, mask and sums    (src/derive3com.f95:502-1043);
 // with a.step, ab3com (src/ab3com.f95:44-61) and the history shift
-__global__ void k3_assemble(const Asm3Args a) {
+__global__ void __launch_bounds__(256, 3) k3_assemble(const Asm3Args a) {
   const size_t n = (size_t)a.Nh * a.Ny * a.Nz;
   for (size_t m = blockIdx.x * (size_t)blockDim.x + threadIdx.x; m < n; m += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(m % a.Nh);
