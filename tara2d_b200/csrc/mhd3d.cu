@@ -825,17 +825,22 @@ int tara3d_step(tara3d* s, int nsteps) {
 int tara3d_time_steps(tara3d* s, int nsteps, float* ms) {
   if (!s || nsteps < 1 || !ms) { set_error("bad argument"); return TARA_EINVAL; }
   TARA_TRY(s->steps(1));  // builds the graph outside the timed region
-  cudaEvent_t e0, e1;
-  TARA_CUDA_TRY(cudaEventCreate(&e0));
-  TARA_CUDA_TRY(cudaEventCreate(&e1));
-  TARA_CUDA_TRY(cudaStreamSynchronize(s->st));
-  TARA_CUDA_TRY(cudaEventRecord(e0, s->st));
-  const int r = s->steps(nsteps);
-  TARA_CUDA_TRY(cudaEventRecord(e1, s->st));
-  TARA_CUDA_TRY(cudaEventSynchronize(e1));
-  TARA_CUDA_TRY(cudaEventElapsedTime(ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // the events are released on every path
+  auto timed = [&]() -> int {
+    TARA_CUDA_TRY(cudaEventCreate(&e0));
+    TARA_CUDA_TRY(cudaEventCreate(&e1));
+    TARA_CUDA_TRY(cudaStreamSynchronize(s->st));
+    TARA_CUDA_TRY(cudaEventRecord(e0, s->st));
+    const int r = s->steps(nsteps);
+    TARA_CUDA_TRY(cudaEventRecord(e1, s->st));
+    TARA_CUDA_TRY(cudaEventSynchronize(e1));
+    TARA_CUDA_TRY(cudaEventElapsedTime(ms, e0, e1));
+    return r;
+  };
+  const int r = timed();
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
   return r;
 }
 int tara3d_launches_per_step(tara3d* s) { return s ? s->launches_per_step() : 0; }
