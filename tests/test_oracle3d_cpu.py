@@ -86,6 +86,17 @@ def test_derive3com_matches_numpy(Nx, Ny, Nz):
         assert rel(got[q], ref[q]) <= 1e-12, (q, rel(got[q], ref[q]))
 
 
+def test_derive3com_matches_numpy_unequal_box():
+    """Lx, Ly, Lz all different (wavenumbers 2 pi i / L per direction)."""
+    Nx, Ny, Nz = 16, 32, 16
+    P = O.Com3Params(Lx=2 * PI, Ly=4 * PI, Lz=PI, mu=0.02, CS=5.0, eta=0.01, dt=1e-4)
+    st = state3(Nx, Ny, Nz, seed=9)
+    got = O.derive3com(Nx, Ny, Nz, P, st)
+    ref = np_derive3com(Nx, Ny, Nz, P, st)
+    for q in range(8):
+        assert rel(got[q], ref[q]) <= 1e-12, (q, rel(got[q], ref[q]))
+
+
 def test_uniform_state_has_zero_rhs():
     N = 16
     Nh = N // 2 + 1
