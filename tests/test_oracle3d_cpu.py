@@ -131,3 +131,14 @@ def test_ab3com_formula():
     for q in range(8):
         ref = u[q] if q == 4 else u[q] + (1.5 * dn[q] - 0.5 * do[q]) * 1e-3
         assert np.array_equal(out[q], ref)
+
+
+@pytest.mark.parametrize("N", [16, 32])
+def test_bench_mask_share_matches_the_oracle(N):
+    """The unmasked share f in bench.py's 3D byte model is the share of modes
+    the oracle's RHS does not zero (the momentum RHS is nonzero on every kept
+    mode except k = 0, where its divergence and k^2 terms vanish)."""
+    import bench
+    d = O.derive3com(N, N, N, params(), state3(N, N, N, seed=N))
+    nonzero = np.count_nonzero(d[1])
+    assert nonzero + 1 == round(bench.mhd3_unmasked_fraction(N) * d[1].size)
