@@ -288,10 +288,12 @@ def run_mhd3d(args):
     """Side workload (not the headline): the 3D path of src/derive3com.f95 +
     src/ab3com.f95 (the driver's AB2 loop, src/main3com.f95:536-600) at N^3 FP64,
     N = --grid3 (256 by default), on one GPU."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0  # a single-GPU side line: under a multi-rank launch rank 0 alone runs it
     import tara2d_b200 as T
     from tara2d_b200 import initial
     N = args.grid3
-    T.set_device(0)
+    T.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     prm = dict(pi=PI, Lx=2 * PI, Ly=2 * PI, Lz=2 * PI, mu=0.01, CS=10.0, eta=0.005, dt=1e-4)
     st0 = initial.mhd3_state(N, N, N, seed=0, noise=1e-4)
     W, K = max(3, args.warmup), max(1, args.steps)
