@@ -212,9 +212,9 @@ def run_ensemble(args):
     one AB2 step.  Compared with the same members run one session at a time."""
     import tara2d_b200 as T
     from tara2d_b200 import initial
-    from tests.gpu_common import coh_kw
     mem = initial.ensemble_members(256, seed=0)
-    params = [T.Params.make(**coh_kw(mux=d["nu"], muy=d["nu"], dt=1e-4)) for d in mem]
+    params = [T.Params.make(Lx=2 * PI, Ly=2 * PI, pi=PI, mux=d["nu"], muy=d["nu"], ms=1.0, CS=3.77, dt=1e-4)
+              for d in mem]
     sizes = [d["N"] for d in mem]
     ens = T.Ensemble(sizes, params, precision=T.FP32)
     for m, d in enumerate(mem):
@@ -350,6 +350,70 @@ def run_mhd3d(args):
     return 0
 
 
+# ------------------------------------------------------------------ per-kernel table
+def kernel_table_bytes(model: str, rk4: bool, S: float) -> dict:
+    """Algorithmic bytes of one launch of each kernel of a model's RHS (every
+    field the kernel must read or write, once; S = one spectral field in the
+    session's precision).  Stepper traffic per field per RHS: AB2 4 S (state
+    and old derivative read, new state and derivative written); RK4 averaged
+    over its stages (3, 4, 4, 2)."""
+    st = (3 + 4 + 4 + 2) / 4.0 if rk4 else 4.0
+    if model == "com":
+        return {"k_col_inv": 12 * S, "k_row_com1": 14 * S, "k_col_rt": 2 * S, "k_row_com2": 7 * S,
+                "k_col_fwd_com": (11 + ((18 + 28 + 28 + 16) / 4.0 if rk4 else 6 * st) + 6) * S}
+    if model == "coh":
+        return {"k_col_inv": 11 * S, "k_row_coh": 11 * S, "k_col_fwd_simple": (3 + 3 * st) * S}
+    return {"k_col_inv": 5 * S, "k_row_vort": 5 * S, "k_col_fwd_vort": (1 + st) * S}
+
+
+def run_kernels(args):
+    """Profiling side line (not the headline): per-kernel launch times of one
+    model's stepping (--model com|coh|csh|css, --grid N, --fp32, --stepper)
+    with CUDA events around every launch, after a graph-replayed timing of
+    the same steps.  States: MHD Orszag-Tang + 1e-3 perturbation on
+    8 <= |k| <= 16 and hydro random phase + 1% density noise, both built on
+    the device; vorticity from a host random-phase state."""
+    import tara2d_b200 as T
+    from tara2d_b200 import initial
+    N = args.grid
+    model = {"com": T.MODEL_COM, "coh": T.MODEL_COH, "csh": T.MODEL_CSH, "css": T.MODEL_CSS}[args.model]
+    rk4 = (args.stepper or ("rk4" if args.model == "com" else "ab2")) == "rk4"
+    stepper = T.STEP_RK4 if rk4 else T.STEP_AB2
+    vpi = T.VORT_PI
+    if model == T.MODEL_COM:
+        p = T.Params.make(Lx=2 * PI, Ly=2 * PI, pi=PI, dt=5e-5 * 1024 / N, mu=5e-4, eta=5e-4, CS=100.0,
+                          spheat=5.0 / 3.0, ms=1.0, mu_0=1.0, kf=1.0, A=0.0, fix_curlB=0)
+    elif model == T.MODEL_COH:
+        p = T.Params.make(Lx=2 * PI, Ly=2 * PI, pi=PI, mux=1e-3, muy=1e-3, ms=1.0, CS=3.77, dt=1e-4 * 128 / N)
+    elif model == T.MODEL_CSH:
+        p = T.Params.make(pi=vpi, Lx=2 * vpi, Ly=2 * vpi, nu=1e-3, dt=1e-3 * 128 / N)
+    else:
+        p = T.Params.make(pi=vpi, Lx=2 * PI, Ly=2 * PI, nu=1e-3, alpha=1.0, dt=1e-3 * 128 / N, **{"lambda": 10.0})
+    W, K = max(1, args.warmup), max(1, args.steps)
+    with T.Session(model, N, N, p, precision=T.FP32 if args.fp32 else T.FP64) as s:
+        if model == T.MODEL_COM:
+            s.set_state_random(T.IC_ORSZAG_TANG, 0, e1=1e-3, e2=1e-3, kmin=8.0, kmax=16.0)
+        elif model == T.MODEL_COH:
+            s.set_state_random(T.IC_RANDOM_PHASE, 0, k0=4.0, e1=0.5, e2=0.01)
+        else:
+            s.set_state(initial.vorticity_random_phase(N, N, seed=0))
+        s.step(stepper, W)
+        ms = s.time_steps(stepper, K)
+        prof, total = s.profile_steps(stepper, K)
+    S = N * (N // 2 + 1) * (8 if args.fp32 else 16)
+    table = kernel_table_bytes(args.model, rk4, S)
+    kernels = {}
+    for k, (t, n) in prof.items():
+        per = t / n
+        b = table.get(k, 0.0)
+        kernels[k] = {"launches": n, "ms_per_launch": per, "share": t / total if total else None,
+                      "alg_bytes_per_launch": b, "alg_GBps": b / (per / 1e3) / 1e9 if b else None}
+    print(json.dumps({"workload": "kernels", "model": args.model, "grid": N,
+                      "precision": "fp32" if args.fp32 else "fp64", "stepper": "rk4" if rk4 else "ab2",
+                      "steps": K, "steps_per_s": K / (ms / 1e3), "S_bytes": S, "kernels": kernels}), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ ranks
 class Ranks:
     """One process per GPU (replicas: the path does not shard).  Rank and
@@ -408,10 +472,13 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=1024, help="grid size (profiling runs only; the metric is at 1024)")
-    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "mhd3d"],
+    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "mhd3d", "kernels"],
                     help="mhd1024: the headline; ensemble: the 256-run batched side workload; "
-                         "mhd3d: the 3D path at --grid3^3")
+                         "mhd3d: the 3D path at --grid3^3; kernels: per-kernel times of --model at --grid")
     ap.add_argument("--grid3", type=int, default=256, help="3D grid size of --workload mhd3d")
+    ap.add_argument("--model", choices=["com", "coh", "csh", "css"], default="com", help="--workload kernels")
+    ap.add_argument("--fp32", action="store_true", help="--workload kernels: FP32 session")
+    ap.add_argument("--stepper", choices=["rk4", "ab2"], default=None, help="--workload kernels")
     args = ap.parse_args()
     global N
     N = args.grid
@@ -421,6 +488,8 @@ def main():
         return run_ensemble(args)
     if args.workload == "mhd3d":
         return run_mhd3d(args)
+    if args.workload == "kernels":
+        return run_kernels(args)
 
     ranks = Ranks("nccl")
     world, rank, local = ranks.world, ranks.rank, ranks.local

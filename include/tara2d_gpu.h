@@ -42,6 +42,7 @@ extern "C" {
 #define TARA_ETIMEOUT (-4)     /* a bounded device wait ran out */
 #define TARA_ENOMEM (-5)       /* device allocation failed */
 #define TARA_EUNSUPPORTED (-6) /* grid size or mode not built */
+#define TARA_ECFL (-7)         /* the time step exceeds the CFL limit (tara_set_cfl) */
 
 /* ---- models ------------------------------------------------------------ */
 #define TARA_MODEL_COH 1 /* compressible isothermal hydro (nk, ukx, uky): derive2coh */
@@ -99,6 +100,44 @@ int tara_launches_per_step(const tara_session* s, int stepper);
  * use per stepper, dropped on tara_set_params); on = 0 launches every kernel
  * from the host instead.  Default: on. */
 int tara_set_graphs(tara_session* s, int on);
+
+/* ---- time-step control and state checks (no counterpart in the reference,
+ * whose drivers step a fixed dt from the INI file, src/main2com.f95:183-193,
+ * and check nothing) ----
+ * CFL control, computed on the device in FP64 at the first RHS evaluation of
+ * every step from the real-space fields the row pass forms anyway:
+ *   rate = max over the grid of (|ux| + c)/dx + (|uy| + c)/dy,
+ *   c = CS (hydro) or sqrt(CS^2 + |B|^2/rho) (MHD, fast magnetosonic speed),
+ *   dt_cfl = cfl / rate.
+ *   TARA_CFL_CHECK: a step whose configured dt exceeds dt_cfl is not taken
+ *     (the state stays as it is) and the session reports TARA_ECFL at its
+ *     next synchronising call; every stepper.
+ *   TARA_CFL_ADAPT: every step uses dt = min(configured dt, dt_cfl); RK4 and
+ *     Euler only (AB2's weights assume a constant step); a step whose dt_cfl
+ *     falls below 1e-6 of the configured dt is not taken (TARA_ECFL).
+ * A rate that is not finite stops the step the same way with TARA_ENAN.
+ * Hydro and MHD models; the vorticity models return TARA_EUNSUPPORTED. */
+#define TARA_CFL_OFF 0
+#define TARA_CFL_CHECK 1
+#define TARA_CFL_ADAPT 2
+int tara_set_cfl(tara_session* s, int mode, double cfl);
+/* Model time advanced by the steps since tara_open (or tara_set_time), and
+ * the dt of the last step (the configured dt when the CFL control is off). */
+int tara_get_time(tara_session* s, double* t, double* dt_last);
+int tara_set_time(tara_session* s, double t);
+/* State checks: tara_set_state and tara_set_history check every uploaded
+ * value, and every tara_step call checks the state it leaves, for values
+ * that are not finite (TARA_ENAN, reported by the call or, for the
+ * asynchronous tara_step, by the next synchronising call). */
+/* Limit, in ns, of every bounded wait of the session's TMA kernels (default
+ * 1 s); a wait that runs out stops its kernel and the session reports
+ * TARA_ETIMEOUT. */
+int tara_set_wait_limit(tara_session* s, long long limit_ns);
+/* Self-test of the bounded wait those kernels use: one CTA waits on an
+ * mbarrier that expects 16 bytes no copy delivers (no copy is issued), with
+ * the given limit (1 us .. 10 s).  Returns what the kernel reports,
+ * TARA_ETIMEOUT when the wait ran out as it must, and the time waited. */
+int tara_selftest_bounded_wait(long long limit_ns, long long* waited_ns);
 
 /* ---- diagnostics, computed on the device from the resident state ----
  * Values (all sums in FP64 whatever the precision; the last two are 0):
@@ -260,7 +299,7 @@ int tara_ens_diagnostics(tara_ensemble* e, int member, double* out, int nout, do
 /* Advance nsteps with a CUDA event recorded before every kernel; returns, per
  * kernel kind (index 0..TARA_NUM_KERNEL_KINDS-1, see tara_kernel_name), the
  * summed device time in ms and the number of launches, plus the total. */
-#define TARA_NUM_KERNEL_KINDS 11
+#define TARA_NUM_KERNEL_KINDS 12
 int tara_profile_steps(tara_session* s, int stepper, int nsteps, double* kernel_ms, int* kernel_launches,
                        float* total_ms);
 const char* tara_kernel_name(int kind);
@@ -294,9 +333,13 @@ int tara_derive2com(const tara_params* p, int Nx, int Ny, const double* const* s
  * device workspace of about 6 MB reserved when the library loads.
  * Nx, Ny must be 16, 32, 64, 128 or 256; anything larger returns
  * TARA_EINVAL.  All calls share the workspace, so calls that overlap on the
- * GPU race; calls on one stream are ordered.  The first call on a device
- * looks up the workspace address and should come before any stream capture.
- * `stream` is a cudaStream_t (NULL: the default stream). */
+ * GPU race; calls on one stream are ordered.  The host-side preparation of
+ * a call (grid tables, kept while Nx, Ny, Lx, Ly and pi stay the same) is
+ * serialised by a lock, so concurrent calls from several host threads are
+ * safe on the host side.  The call runs no TMA tile loads and no bounded
+ * device waits: its return value is its whole status.  The first call on a
+ * device looks up the workspace address and should come before any stream
+ * capture.  `stream` is a cudaStream_t (NULL: the default stream). */
 int tara_derive2coh_noalloc(const tara_params* p, int Nx, int Ny, const double* nk, const double* ukx,
                             const double* uky, double* dn_dt, double* dux_dt, double* duy_dt, void* stream);
 

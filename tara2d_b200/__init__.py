@@ -20,13 +20,14 @@ from . import initial  # noqa: F401  (seeded initial conditions)
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libtara2d_b200.so")
 
-OK, EINVAL, ECUDA, ENAN, ETIMEOUT, ENOMEM, EUNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
+OK, EINVAL, ECUDA, ENAN, ETIMEOUT, ENOMEM, EUNSUPPORTED, ECFL = 0, -1, -2, -3, -4, -5, -6, -7
+CFL_OFF, CFL_CHECK, CFL_ADAPT = 0, 1, 2
 MODEL_COH, MODEL_COM, MODEL_CSH, MODEL_CSS = 1, 2, 3, 4
 FP64, FP32 = 0, 1
 STEP_AB2, STEP_RK4, STEP_EULER = 0, 1, 2
 LEGACY_REFERENCE, LEGACY_CORRECT = 0, 1
 SUPPORTED_N = (16, 32, 64, 128, 256, 384, 512, 1024, 2048, 4096)
-NUM_KERNEL_KINDS = 11
+NUM_KERNEL_KINDS = 12
 DIAG_VALUES = 8
 NFIELDS = {MODEL_COH: 3, MODEL_COM: 6, MODEL_CSH: 1, MODEL_CSS: 1}
 PI = 3.14159265358979323846
@@ -36,7 +37,9 @@ VORT_PI = float(np.float32(3.1428))
 
 
 class TaraError(RuntimeError):
-    pass
+    def __init__(self, msg: str, status: int = 0):
+        super().__init__(msg)
+        self.status = status
 
 
 class IcDesc(C.Structure):
@@ -150,6 +153,11 @@ def lib():
         L.tara_diagnostics.argtypes = [P, P, I, P, I]
         L.tara_run_recorded.argtypes = [P, I, I, I, P]
         L.tara_set_css_box.argtypes = [D, D, D]
+        L.tara_set_cfl.argtypes = [P, I, D]
+        L.tara_get_time.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.tara_set_time.argtypes = [P, D]
+        L.tara_set_wait_limit.argtypes = [P, C.c_longlong]
+        L.tara_selftest_bounded_wait.argtypes = [C.c_longlong, C.POINTER(C.c_longlong)]
         _lib = L
     return _lib
 
@@ -160,7 +168,15 @@ def last_error() -> str:
 
 def check(status: int, what: str = "") -> None:
     if status != OK:
-        raise TaraError(f"{what} failed with status {status}: {last_error()}")
+        raise TaraError(f"{what} failed with status {status}: {last_error()}", status)
+
+
+def selftest_bounded_wait(limit_ns: int):
+    """tara_selftest_bounded_wait: (status, ns waited) of a kernel whose
+    bounded mbarrier wait must run out (status ETIMEOUT)."""
+    waited = C.c_longlong()
+    st = lib().tara_selftest_bounded_wait(int(limit_ns), C.byref(waited))
+    return st, waited.value
 
 
 def _ptrs(arrs):
@@ -309,6 +325,22 @@ class Session:
     def set_state(self, fields) -> None:
         a = self._fields_in(fields)
         check(lib().tara_set_state(self._h, _ptrs(a)), "tara_set_state")
+
+    def set_cfl(self, mode: int, cfl: float = 0.0) -> None:
+        """CFL control (CFL_OFF, CFL_CHECK, CFL_ADAPT) with CFL number cfl."""
+        check(lib().tara_set_cfl(self._h, mode, cfl), "tara_set_cfl")
+
+    def time(self):
+        """(model time advanced so far, dt of the last step)."""
+        t, dt = C.c_double(), C.c_double()
+        check(lib().tara_get_time(self._h, C.byref(t), C.byref(dt)), "tara_get_time")
+        return t.value, dt.value
+
+    def set_time(self, t: float) -> None:
+        check(lib().tara_set_time(self._h, t), "tara_set_time")
+
+    def set_wait_limit(self, ns: int) -> None:
+        check(lib().tara_set_wait_limit(self._h, int(ns)), "tara_set_wait_limit")
 
     def get_state(self):
         out = self._fields_out()

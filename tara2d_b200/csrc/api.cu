@@ -112,6 +112,7 @@ struct SessionT : tara_session {
     drop_graphs();
     g.release(); u.release(); unew.release(); dold.release(); acc.release(); us.release(); us2.release();
     tmp.release(); dw.release(); closf.release();
+    if (cfl_dev) cudaFree(cfl_dev);
     if (rbuf) cudaFree(rbuf);
     if (rstage) cudaFree(rstage);
     stage.release(); cw.release(); mw.release(); vw.release();
@@ -127,6 +128,12 @@ struct SessionT : tara_session {
     TARA_TRY(us2.alloc(g, nf, st));
     TARA_TRY(unew.alloc(g, nf, st));
     TARA_TRY(tmp.alloc(g, nf, st));
+    if (cudaMalloc(&cfl_dev, sizeof(CflDev)) != cudaSuccess) {
+      cfl_dev = nullptr;
+      set_error("cudaMalloc of the CFL state failed");
+      return TARA_ENOMEM;
+    }
+    TARA_CUDA_TRY(cudaMemsetAsync(cfl_dev, 0, sizeof(CflDev), st));
     if (sizeof(T) != sizeof(double)) {
       // staging as complex128 [Ny][Nh] (host layout, no pitch)
       stage.elems = (size_t)Nh * Ny;
@@ -183,10 +190,72 @@ struct SessionT : tara_session {
       const int zero = 0;
       cudaMemcpyAsync(g.tb.status, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
       cudaStreamSynchronize(st);
-      set_error("a bounded wait for a TMA tile load ran out in a kernel");
+      switch (v) {
+        case TARA_ENAN: set_error("a value that is not finite was found (state, history or CFL rate)"); break;
+        case TARA_ECFL: set_error("the time step exceeds the CFL limit; the step was not taken"); break;
+        default: set_error("a bounded wait for a TMA tile load ran out in a kernel"); break;
+      }
       return v;
     }
     return TARA_OK;
+  }
+
+  // ---- CFL control (first RHS of every step) and time
+  CflDev* cfl_dev = nullptr;
+  int cfl_mode = CFL_OFF;
+  double cfl_number = 0.0;
+  double t_off = 0.0;   // model time of the steps taken with the CFL control off
+  CflCfg cur_cfl{};     // settings of the RHS being launched
+  CflCfg cfl_cfg() const {
+    if (cfl_mode == CFL_OFF) return CflCfg{};
+    CflCfg c{};
+    c.dev = cfl_dev;
+    c.mode = cfl_mode;
+    c.number = cfl_number;
+    c.dt = p.dt;
+    c.idx = (double)Nx / p.Lx;
+    c.idy = (double)Ny / p.Ly;
+    c.cs2 = p.CS * p.CS;
+    return c;
+  }
+  int set_cfl(int mode, double number) override {
+    if (model != TARA_MODEL_COH && model != TARA_MODEL_COM) {
+      set_error("the CFL control is defined for the hydro and MHD models");
+      return TARA_EUNSUPPORTED;
+    }
+    if (mode != CFL_OFF && mode != CFL_CHECK && mode != CFL_ADAPT) { set_error("unknown CFL mode"); return TARA_EINVAL; }
+    if (mode != CFL_OFF && !(number > 0.0)) { set_error("the CFL number must be positive"); return TARA_EINVAL; }
+    drop_graphs();  // the graphs hold the CFL settings in their kernel arguments
+    cfl_mode = mode;
+    cfl_number = number;
+    return TARA_OK;
+  }
+  int get_time(double* t, double* dt) override {
+    CflDev d{};
+    TARA_CUDA_TRY(cudaMemcpyAsync(&d, cfl_dev, sizeof(CflDev), cudaMemcpyDeviceToHost, st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    if (t) *t = t_off + d.t;
+    if (dt) *dt = cfl_mode == CFL_OFF ? p.dt : d.dt;
+    return TARA_OK;
+  }
+  int set_time(double t) override {
+    double td = 0.0;
+    TARA_CUDA_TRY(cudaMemcpyAsync(&td, &cfl_dev->t, sizeof(double), cudaMemcpyDeviceToHost, st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    t_off = t - td;
+    return TARA_OK;
+  }
+  int set_wait_limit(long long ns) override {
+    if (ns < 1000) { set_error("wait limit below 1 us"); return TARA_EINVAL; }
+    drop_graphs();
+    g.tb.wait_ns = (unsigned long long)ns;
+    return TARA_OK;
+  }
+  // TARA_ENAN into the status word when a value of these fields is not finite
+  int check_finite(FieldPool<T>& f) {
+    Cx<T>* q[6];
+    for (int k = 0; k < nf; k++) q[k] = f[k];
+    return launch_finite_check(g, q, nf, st);
   }
 
   int h2d(const double* h, Cx<T>* d) {
@@ -223,8 +292,9 @@ struct SessionT : tara_session {
     if (!h) { set_error("null field array"); return TARA_EINVAL; }
     if (which == 0) h_for = nullptr;
     for (int f = 0; f < nf; f++) TARA_TRY(h2d(h[f], pool(which)[f]));
+    TARA_TRY(check_finite(pool(which)));
     TARA_CUDA_TRY(cudaStreamSynchronize(st));
-    return TARA_OK;
+    return device_status();
   }
   int get_fields(int which, double* const* h) override {
     if (!h) { set_error("null field array"); return TARA_EINVAL; }
@@ -234,7 +304,9 @@ struct SessionT : tara_session {
 
   int rhs(Cx<T>* const* in, const StepArgs<T>& s) {
     switch (model) {
-      case TARA_MODEL_COH: return coh_rhs(g, cw, cohp, in, s, st);
+      case TARA_MODEL_COH:
+        cohp.cfl = cur_cfl;
+        return coh_rhs(g, cw, cohp, in, s, st);
       case TARA_MODEL_COM: {
         if constexpr (sizeof(T) == sizeof(double)) {
           if (clos) {  // the learned closure's stress/EMF spectra for this RHS input
@@ -246,6 +318,7 @@ struct SessionT : tara_session {
         // the y-inverse of this input; stepping RHS write it for the next input
         comp.skip_inv = h_for == (const void*)in[0];
         comp.fuse_inv = s.mode != STEP_RHS;
+        comp.cfl = cur_cfl;
         const int r = com_rhs(g, mw, comp, in, s, st);
         if (s.mode == STEP_RHS) h_for = in[0];
         else if (s.mode == STEP_RK4 && s.stage < 3) h_for = s.us[0];
@@ -286,6 +359,7 @@ struct SessionT : tara_session {
     StepArgs<T> s{};
     s.mode = mode;
     s.dt = (T)p.dt;
+    s.scale = (cfl_mode != CFL_OFF && mode != STEP_RHS) ? &cfl_dev->scale : nullptr;
     for (int f = 0; f < nf; f++) {
       s.out[f] = tmp[f];
       s.u[f] = u[f];
@@ -365,6 +439,17 @@ struct SessionT : tara_session {
       set_error("unknown stepper");
       return TARA_EINVAL;
     }
+    if (cfl_mode == CFL_ADAPT && stepper == TARA_STEP_AB2) {
+      set_error("the adaptive CFL step needs RK4 or Euler (AB2's weights assume a constant dt)");
+      return TARA_EINVAL;
+    }
+    TARA_TRY(step_launch(stepper, n));
+    if (cfl_mode == CFL_OFF) t_off += n * p.dt;
+    // the state this call leaves must be finite (reported at the next
+    // synchronising call)
+    return n > 0 ? check_finite(u) : TARA_OK;
+  }
+  int step_launch(int stepper, int n) {
     int done = 0;
     if (model == TARA_MODEL_COM && n >= 1 && h_for != (const void*)u[0]) {
       // one step with the column-inverse pass; after it mw.H holds the inverse
@@ -387,7 +472,10 @@ struct SessionT : tara_session {
       Cx<T>* in_u[6];
       for (int f = 0; f < nf; f++) in_u[f] = u[f];
       if (stepper == TARA_STEP_AB2 || stepper == TARA_STEP_EULER) {
-        TARA_TRY(rhs(in_u, base_args(stepper == TARA_STEP_AB2 ? STEP_AB2 : STEP_EULER)));
+        cur_cfl = cfl_cfg();
+        const int r = rhs(in_u, base_args(stepper == TARA_STEP_AB2 ? STEP_AB2 : STEP_EULER));
+        cur_cfl = CflCfg{};
+        TARA_TRY(r);
       } else {
         // classical RK4; weights and stage offsets as in the oracle:
         // acc = u + (w dt/6) k1 ; us = u + (c dt) k ; u_new = acc + (dt/6) k4
@@ -403,7 +491,10 @@ struct SessionT : tara_session {
             in[f] = s == 0 ? u[f] : (*ping[(s - 1) & 1])[f];
             a.us[f] = (*ping[s & 1])[f];
           }
-          TARA_TRY(rhs(in, a));
+          cur_cfl = s == 0 ? cfl_cfg() : CflCfg{};
+          const int r = rhs(in, a);
+          cur_cfl = CflCfg{};
+          TARA_TRY(r);
         }
       }
       std::swap(u, unew);
@@ -907,6 +998,14 @@ int tara_set_graphs(tara_session* s, int on) {
   if (!s) return TARA_EINVAL;
   s->set_graphs(on != 0);
   return TARA_OK;
+}
+int tara_set_cfl(tara_session* s, int mode, double cfl) { return s ? s->fail_if(s->set_cfl(mode, cfl)) : TARA_EINVAL; }
+int tara_get_time(tara_session* s, double* t, double* dt_last) {
+  return s ? s->fail_if(s->get_time(t, dt_last)) : TARA_EINVAL;
+}
+int tara_set_time(tara_session* s, double t) { return s ? s->fail_if(s->set_time(t)) : TARA_EINVAL; }
+int tara_set_wait_limit(tara_session* s, long long limit_ns) {
+  return s ? s->fail_if(s->set_wait_limit(limit_ns)) : TARA_EINVAL;
 }
 int tara_num_shells(tara_session* s) { return s ? s->num_shells() : 0; }
 int tara_diagnostics(tara_session* s, double* out, int nout, double* Ek, int nbins) {

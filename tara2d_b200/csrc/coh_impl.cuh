@@ -24,6 +24,7 @@ template <class T> struct RowCohArgs {
   Cx<T>* X[3];
   T mux, muy, cs2;
   int rb;
+  CflRow cfl;  // cfl.lam set: fold the rows' largest signal-speed rate into it
 };
 
 // One group per transform.  Phase 1: eleven c2r in eleven groups (each
@@ -84,6 +85,10 @@ __device__ __forceinline__ void row_coh_rows(const RowCohArgs<T>& a, int y0, Cx<
   // phase 2: products                              (:153-165)
   //   NLn = ux dn/dx + uy dn/dy + n (dux/dx + duy/dy)
   //   Fx  = (ux dux/dx + uy dux/dy) + visc_x/n + CS^2 (dn/dx)/n   (+ same for y)
+  // CFL control: largest (|ux| + CS)/dx + (|uy| + CS)/dy of the points, in FP64
+  const bool cfl = a.cfl.lam != nullptr;
+  const double cs = cfl ? sqrt(a.cfl.cs2) : 0.0;
+  double cmax = 0.0;
   for (int m = th.g * NTR + th.lane; m < M; m += G * NTR) {
     T q[11][2];
 #pragma unroll
@@ -103,7 +108,10 @@ __device__ __forceinline__ void row_coh_rows(const RowCohArgs<T>& a, int y0, Cx<
     }
 #pragma unroll
     for (int f = 0; f < 3; f++) arr(f)[m] = cx<T>(o[f][0], o[f][1]);
+    if (cfl)
+      for (int h = 0; h < 2; h++) cmax = nan_max(cmax, cfl_rate(q[1][h], q[2][h], cs, a.cfl.idx, a.cfl.idy));
   }
+  if (cfl) cfl_fold(cmax, a.cfl.lam);
   __syncthreads();
   // phase 3: three r2c along x                     (:172-197, merged by linearity)
   if (th.g < 3) {
@@ -162,8 +170,13 @@ int coh_rhs(const Grid<T>& g, CohWork<T>& w, const CohParamsT<T>& p, Cx<T>* cons
   ra.mux = p.mux;
   ra.muy = p.muy;
   ra.cs2 = p.cs2;
+  if (p.cfl.dev) ra.cfl = CflRow{&p.cfl.dev->lam, p.cfl.idx, p.cfl.idy, p.cfl.cs2};
   prof_mark(g.prof, st, KK_ROW_COH);
   TARA_DISPATCH_LEN(g.Nx, launch_row_coh, ra, g.Ny, st)
+  if (p.cfl.dev) {  // dt of this step, before the stepper update reads it
+    prof_mark(g.prof, st, KK_CFL);
+    TARA_TRY(launch_cfl_update(p.cfl, g.tb.status, st));
+  }
 
   ColFwdSimpleArgs<T> cf{};
   cf.tb = g.tb;

@@ -56,6 +56,7 @@ template <class T> struct RowCom1Args {
   Cx<T>* X[11];
   T cs2;
   int rb;
+  CflRow cfl;  // cfl.lam set: fold the rows' largest signal-speed rate into it
 };
 
 template <class T, int M, int P, bool LOW>
@@ -84,6 +85,23 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
     });
   }
   __syncthreads();
+  if (a.cfl.lam) {
+    // CFL control: largest (|ux| + cf)/dx + (|uy| + cf)/dy of the CTA's
+    // points, cf = sqrt(CS^2 + |B|^2/rho) (fast magnetosonic speed), in FP64
+    double m = 0.0;
+    for (int n = th.g * NTR + th.lane; n < M; n += G * NTR) {
+      const Cx<T> r = f[0][n], mx = f[1][n], my = f[2][n], bx = f[4][n], by = f[5][n];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const double rho = h ? r.y : r.x;
+        const double ux = (h ? mx.y : mx.x) / rho, uy = (h ? my.y : my.x) / rho;
+        const double b2 = h ? (double)bx.y * bx.y + (double)by.y * by.y : (double)bx.x * bx.x + (double)by.x * by.x;
+        const double c = sqrt(a.cfl.cs2 + b2 / rho);
+        m = nan_max(m, cfl_rate(ux, uy, c, a.cfl.idx, a.cfl.idy));
+      }
+    }
+    cfl_fold(m, a.cfl.lam);
+  }
   // flux q at one point                                                (:105-106, :193-213)
   const T cs2 = a.cs2;
   auto flux = [&](int qq, T rho, T mx, T my, T E, T bx, T by) -> T {
@@ -513,8 +531,13 @@ int com_rhs(const Grid<T>& g, ComWork<T>& w, const ComParamsT<T>& p, Cx<T>* cons
   for (int q = 0; q < 6; q++) r1.H[q] = w.H[q];
   for (int q = 0; q < 11; q++) r1.X[q] = w.X[q];
   r1.cs2 = p.cs2;
+  if (p.cfl.dev) r1.cfl = CflRow{&p.cfl.dev->lam, p.cfl.idx, p.cfl.idy, p.cfl.cs2};
   prof_mark(g.prof, st, KK_ROW_COM1);
   TARA_DISPATCH_LEN(g.Nx, launch_row_com1, r1, g.Ny, st)
+  if (p.cfl.dev) {  // dt of this step, before any stepper update reads it
+    prof_mark(g.prof, st, KK_CFL);
+    TARA_TRY(launch_cfl_update(p.cfl, g.tb.status, st));
+  }
   if (forcing) {
     RowForceArgs<T> rf{};
     rf.tb = g.tb;

@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(CB * L / P, 1) k_col_inv_tma(const __grid_cons
       fence_proxy_async_smem();
       issue(next, b ^ 1);
     }
-    const bool ok = mbar_wait_bounded(&bars[b], parity);
+    const bool ok = mbar_wait_bounded(&bars[b], parity, a.tb.wait_ns);
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
@@ -217,8 +217,8 @@ __global__ void __launch_bounds__(CB * L / P, 1) k_col_inv_tma(const __grid_cons
     // record the failure, then let the loads still in flight land (bounded)
     if (tid == 0) atomicExch(a.tb.status, TARA_ETIMEOUT);
     const int b = it & 1;
-    mbar_wait_bounded(&bars[b], (it >> 1) & 1);
-    if (item + (int)gridDim.x < nitems) mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1);
+    mbar_wait_bounded(&bars[b], (it >> 1) & 1, a.tb.wait_ns);
+    if (item + (int)gridDim.x < nitems) mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1, a.tb.wait_ns);
   }
 }
 
@@ -237,12 +237,55 @@ template <class T> struct StepArgs {
   Cx<T>* dold[6]; // AB2 history, replaced by the new derivative (same element, same thread)
   Cx<T>* acc[6];  // RK4 accumulator
   Cx<T>* us[6];   // RK4 next stage input; never aliases the current stage input
+  // CFL control (nullptr: off): dt, wa and cs are multiplied by *scale, the
+  // factor the CFL update of this step wrote on the device (1 leaves them
+  // exactly as given; 0 stops the step)
+  const double* scale;
+};
+
+// Device state of the CFL control of a session (see k_cfl_update).
+struct CflDev {
+  unsigned long long lam;  // max over the grid of the signal-speed rate, as the bits of a non-negative double
+  double scale;            // dt of this step / the configured dt
+  double t;                // model time advanced under CFL control
+  double dt;               // dt of the last step
+};
+
+// Folds one thread's largest signal-speed rate m into *lam: a maximum over
+// the threads of the warp that call it together (their bit patterns: a
+// non-negative double orders like its bits, and a NaN or inf exceeds every
+// finite value), then one atomicMax per warp.  Partial warps are fine.
+__device__ __forceinline__ double nan_max(double a, double b) { return (b > a || b != b) ? b : a; }
+__device__ __forceinline__ void cfl_fold(double m, unsigned long long* lam) {
+  const unsigned mask = __activemask();
+  const unsigned long long b = (unsigned long long)__double_as_longlong(m);
+  const unsigned hi = (unsigned)(b >> 32), lo = (unsigned)(b & 0xffffffffu);
+  const unsigned mhi = __reduce_max_sync(mask, hi);
+  const unsigned mlo = __reduce_max_sync(mask, hi == mhi ? lo : 0u);
+  if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(lam, ((unsigned long long)mhi << 32) | mlo);
+}
+// Signal-speed rate of one grid point, (|ux| + c)/dx + (|uy| + c)/dy.
+__device__ __forceinline__ double cfl_rate(double ux, double uy, double c, double idx, double idy) {
+  return (fabs(ux) + c) * idx + (fabs(uy) + c) * idy;
+}
+// CFL arguments of a row pass (lam == nullptr: not computed).
+struct CflRow {
+  unsigned long long* lam;
+  double idx, idy;  // 1/dx, 1/dy
+  double cs2;       // squared sound speed
 };
 
 // d = derivative of field f at element idx.  Operation order follows
 // src/ab2coh.f95:22 / src/ab2com.f95:69 and src/euler2coh.f95:104.
 template <class T>
 __device__ __forceinline__ void step_apply(const StepArgs<T>& s, int f, size_t idx, Cx<T> d) {
+  T dt = s.dt, wa = s.wa, cs = s.cs;
+  if (s.scale) {
+    const T sc = (T)*s.scale;
+    dt *= sc;
+    wa *= sc;
+    cs *= sc;
+  }
   switch (s.mode) {
     case STEP_RHS:
       st(s.out[f] + idx, d);
@@ -251,29 +294,29 @@ __device__ __forceinline__ void step_apply(const StepArgs<T>& s, int f, size_t i
       Cx<T> old = ld(s.dold[f] + idx);
       Cx<T> u = ld(s.u[f] + idx);
       Cx<T> inc = rmul((T)1.5, d) - rmul((T)0.5, old);
-      st(s.unew[f] + idx, u + rmul(s.dt, inc));
+      st(s.unew[f] + idx, u + rmul(dt, inc));
       st(s.dold[f] + idx, d);
       break;
     }
     case STEP_EULER: {
       Cx<T> u = ld(s.u[f] + idx);
-      st(s.unew[f] + idx, u + rmul(s.dt, d));
+      st(s.unew[f] + idx, u + rmul(dt, d));
       st(s.dold[f] + idx, d);
       break;
     }
     default: {  // RK4
       if (s.stage == 0) {
         Cx<T> u = ld(s.u[f] + idx);
-        st(s.acc[f] + idx, u + rmul(s.wa, d));
-        st(s.us[f] + idx, u + rmul(s.cs, d));
+        st(s.acc[f] + idx, u + rmul(wa, d));
+        st(s.us[f] + idx, u + rmul(cs, d));
       } else if (s.stage < 3) {
         Cx<T> u = ld(s.u[f] + idx);
         Cx<T> a = ld(s.acc[f] + idx);
-        st(s.acc[f] + idx, a + rmul(s.wa, d));
-        st(s.us[f] + idx, u + rmul(s.cs, d));
+        st(s.acc[f] + idx, a + rmul(wa, d));
+        st(s.us[f] + idx, u + rmul(cs, d));
       } else {
         Cx<T> a = ld(s.acc[f] + idx);
-        st(s.unew[f] + idx, a + rmul(s.wa, d));
+        st(s.unew[f] + idx, a + rmul(wa, d));
       }
       break;
     }
@@ -299,6 +342,13 @@ __device__ __forceinline__ void step_apply_n(const StepArgs<T>& s, int f, POS&& 
     }
     return;
   }
+  T dt = s.dt, wa = s.wa, cs = s.cs;
+  if (s.scale) {
+    const T sc = (T)*s.scale;
+    dt *= sc;
+    wa *= sc;
+    cs *= sc;
+  }
   const bool rk4 = s.mode == STEP_RK4;
   const bool need0 = s.mode == STEP_AB2 || (rk4 && s.stage > 0);  // AB2 history or RK4 accumulator
   const bool need1 = !rk4 || s.stage < 3;                          // state
@@ -322,31 +372,31 @@ __device__ __forceinline__ void step_apply_n(const StepArgs<T>& s, int f, POS&& 
     Cx<T> nv = cx<T>(0, 0);
     if (s.mode == STEP_AB2) {
       const Cx<T> inc = rmul((T)1.5, de) - rmul((T)0.5, x0[e]);
-      nv = x1[e] + rmul(s.dt, inc);
+      nv = x1[e] + rmul(dt, inc);
       if (ok) {
         st(s.unew[f] + idx, nv);
         st(s.dold[f] + idx, de);
       }
     } else if (s.mode == STEP_EULER) {
-      nv = x1[e] + rmul(s.dt, de);
+      nv = x1[e] + rmul(dt, de);
       if (ok) {
         st(s.unew[f] + idx, nv);
         st(s.dold[f] + idx, de);
       }
     } else if (s.stage == 0) {
-      nv = x1[e] + rmul(s.cs, de);
+      nv = x1[e] + rmul(cs, de);
       if (ok) {
-        st(s.acc[f] + idx, x1[e] + rmul(s.wa, de));
+        st(s.acc[f] + idx, x1[e] + rmul(wa, de));
         st(s.us[f] + idx, nv);
       }
     } else if (s.stage < 3) {
-      nv = x1[e] + rmul(s.cs, de);
+      nv = x1[e] + rmul(cs, de);
       if (ok) {
-        st(s.acc[f] + idx, x0[e] + rmul(s.wa, de));
+        st(s.acc[f] + idx, x0[e] + rmul(wa, de));
         st(s.us[f] + idx, nv);
       }
     } else {
-      nv = x0[e] + rmul(s.wa, de);
+      nv = x0[e] + rmul(wa, de);
       if (ok) st(s.unew[f] + idx, nv);
     }
     if (nxt) nxt[e] = ok ? nv : cx<T>(0, 0);
@@ -441,7 +491,7 @@ inline void col_inv_dispatch(const ColInvArgs<T>& a, int njobs, cudaStream_t st)
   t.ntiles = (a.tb.Nh + CB - 1) / CB;
   // two column tiles must fit in shared memory (not so for the longest columns)
   constexpr bool fits = LY::template bytes<T>() <= 220 * 1024;
-  bool maps_ok = fits && (a.tb.ld * sizeof(Cx<T>)) % 16 == 0 && (2 * CB * sizeof(T)) % 16 == 0;
+  bool maps_ok = fits && !a.tb.no_tma && (a.tb.ld * sizeof(Cx<T>)) % 16 == 0 && (2 * CB * sizeof(T)) % 16 == 0;
   for (int q = 0; q < njobs && maps_ok; q++) {
     t.job[q] = a.job[q];
     maps_ok = make_col_tile_map<T>(&t.map[q], a.job[q].src, a.tb.ld, a.tb.Ny, CB, LY::BOX) == TARA_OK;

@@ -692,6 +692,8 @@ struct tara3d {
     tb.nn_pow2 = 1;  // every supported size is a power of two
     tb.status = (int*)(b + o_status);
     tb.sm_count = sms;
+    tb.no_tma = 0;
+    tb.wait_ns = 1000000000ull;
     return TARA_OK;
   }
 

@@ -7,8 +7,30 @@
 
 namespace tara {
 
+// ---- CFL control and state checks (guard.cu) ----
+enum : int { CFL_OFF = TARA_CFL_OFF, CFL_CHECK = TARA_CFL_CHECK, CFL_ADAPT = TARA_CFL_ADAPT };
+// CFL settings of one RHS evaluation: dev == nullptr, or a RHS that is not
+// the first of its step, computes no rate.
+struct CflCfg {
+  CflDev* dev;
+  int mode;
+  double number;    // CFL number C: dt_cfl = C / max over the grid of the rate
+  double dt;        // configured dt (the largest step)
+  double idx, idy;  // 1/dx, 1/dy
+  double cs2;       // squared sound speed
+};
+// dt of this step from the folded rate (one thread): writes dev->scale, ->dt,
+// advances ->t, clears ->lam; TARA_ECFL / TARA_ENAN into *status.
+int launch_cfl_update(const CflCfg& c, int* status, cudaStream_t st);
+// TARA_ENAN into tb.status when a value of the nf fields is not finite.
+template <class T>
+int launch_finite_check(const Grid<T>& g, Cx<T>* const* f, int nf, cudaStream_t st);
+
 // ---- compressible isothermal hydro, src/derive2coh.f95 ----
-template <class T> struct CohParamsT { T mux, muy, cs2; };
+template <class T> struct CohParamsT {
+  T mux, muy, cs2;
+  CflCfg cfl;
+};
 template <class T> struct CohWork {
   FieldPool<T> H;  // 8 half-real fields: n, iky n, ux, iky ux, ky2 ux, uy, iky uy, ky2 uy
   FieldPool<T> X;  // 3 x-transformed rows: NLn, momentum-x, momentum-y
@@ -36,6 +58,7 @@ template <class T> struct ComParamsT {
   int closure;
   const Cx<T>* clos[4];
   int skip_inv, fuse_inv;
+  CflCfg cfl;
 };
 template <class T> struct ComWork {
   FieldPool<T> H;  // half-real: rho, rho_ux, rho_uy, E, Bx, By, d(uy)/dy, [iky Bx, ikx By]

@@ -21,11 +21,21 @@
 //     the GPU (different streams without ordering) race and give wrong
 //     results; calls on one stream are ordered and safe.  Each call writes
 //     every workspace element it later reads, so nothing needs clearing.
+//   * The grid tables (twiddles, wavenumbers, dealiasing cut-offs) are built
+//     on the host into one fixed-size static structure, rebuilt only when
+//     (Nx, Ny, Lx, Ly, pi) change, and reach the workspace as the by-value
+//     parameter of a small copy kernel (no host-to-device memcpy).  A mutex
+//     serialises that host-side preparation, so calls from several host
+//     threads do not corrupt each other's tables on the host.
+//   * The column passes run the register-staged kernels (no TMA tile loads,
+//     hence no bounded waits and no device status word to read back): every
+//     failure of a call is reported by its return value.
 //   * The first call on a device looks up the workspace's device address
 //     (cudaGetSymbolAddress) for that device; make that first call before
 //     any stream capture begins.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include "models.h"
 
 namespace {
@@ -44,29 +54,109 @@ static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 static void* g_scratch_addr[kMaxDevices] = {nullptr};
 
-// Host staging of the tables: fixed-size, so that building them allocates nothing.
-static Cx<double> h_tw_col[kMaxN];
-static Cx<double> h_tw_row[kMaxN / 2];
-static Cx<double> h_tw_real[kMaxN / 2 + 1];
-static double h_kx[kMaxNh];
-static double h_ky[kMaxN];
-static int h_cut[kMaxN];
-static unsigned char h_tables[kTableBytes];
+// Grid tables of one call, built on the host.  Fixed size, so that building
+// them allocates nothing; passed by value to k_noalloc_tables (about 12 KB of
+// kernel parameters).
+struct NoallocTables {
+  Cx<double> tw_col[kMaxN];
+  Cx<double> tw_row[kMaxN / 2];
+  Cx<double> tw_real[kMaxN / 2 + 1];
+  double kx[kMaxNh];
+  double ky[kMaxN];
+  int cut[kMaxN];
+};
+// Byte offsets of the tables inside the workspace's table region (each on a
+// 256-byte boundary).
+constexpr size_t al256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kOffTwCol = 0;
+constexpr size_t kOffTwRow = al256(kOffTwCol + sizeof(Cx<double>) * kMaxN);
+constexpr size_t kOffTwReal = al256(kOffTwRow + sizeof(Cx<double>) * (kMaxN / 2));
+constexpr size_t kOffKx = al256(kOffTwReal + sizeof(Cx<double>) * (kMaxN / 2 + 1));
+constexpr size_t kOffKy = al256(kOffKx + sizeof(double) * kMaxNh);
+constexpr size_t kOffCut = al256(kOffKy + sizeof(double) * kMaxN);
+constexpr size_t kOffStatus = kTableBytes - 256;
+static_assert(kOffCut + sizeof(int) * kMaxN <= kOffStatus, "tables exceed the workspace's table region");
 
-int scratch_address(void** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) {
-    tara::set_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    return TARA_ECUDA;
+// Host cache of the last tables built and the lock that serialises the
+// host-side preparation (workspace lookup, table build, table upload).
+static std::mutex g_mu;
+static NoallocTables g_tab;
+static int g_key_n[2] = {0, 0};
+static double g_key_d[3] = {0, 0, 0};
+
+__global__ void k_noalloc_tables(const NoallocTables t, unsigned char* dtab, int Ny, int M, int Nh) {
+  Cx<double>* twc = reinterpret_cast<Cx<double>*>(dtab + kOffTwCol);
+  Cx<double>* twr = reinterpret_cast<Cx<double>*>(dtab + kOffTwRow);
+  Cx<double>* twre = reinterpret_cast<Cx<double>*>(dtab + kOffTwReal);
+  double* kx = reinterpret_cast<double*>(dtab + kOffKx);
+  double* ky = reinterpret_cast<double*>(dtab + kOffKy);
+  int* cut = reinterpret_cast<int*>(dtab + kOffCut);
+  for (int m = threadIdx.x; m < Ny; m += blockDim.x) {
+    twc[m] = t.tw_col[m];
+    ky[m] = t.ky[m];
+    cut[m] = t.cut[m];
   }
+  for (int m = threadIdx.x; m <= M; m += blockDim.x) {
+    if (m < M) twr[m] = t.tw_row[m];
+    twre[m] = t.tw_real[m];
+  }
+  for (int i = threadIdx.x; i < Nh; i += blockDim.x) kx[i] = t.kx[i];
+  if (threadIdx.x == 0) *reinterpret_cast<int*>(dtab + kOffStatus) = TARA_OK;
+}
+
+// Builds the tables of (Nx, Ny, Lx, Ly, pi) into g_tab with the reference
+// formulas (kx, ky: src/derive2coh.f95:58-86; 2/3 rule: :208-212), unless
+// g_tab holds them already.  Called with g_mu held.
+void build_tables(int Nx, int Ny, const tara_params* p) {
+  if (g_key_n[0] == Nx && g_key_n[1] == Ny && g_key_d[0] == p->Lx && g_key_d[1] == p->Ly && g_key_d[2] == p->pi)
+    return;
+  const int Nh = Nx / 2 + 1, M = Nx / 2;
+  NoallocTables& t = g_tab;
+  for (int m = 0; m < Ny; m++) {
+    long double c, s;
+    tara::twiddle(m, Ny, c, s);
+    t.tw_col[m] = tara::cx<double>((double)c, (double)s);
+  }
+  for (int m = 0; m < M; m++) {
+    long double c, s;
+    tara::twiddle(m, M, c, s);
+    t.tw_row[m] = tara::cx<double>((double)c, (double)s);
+  }
+  for (int m = 0; m <= M; m++) {
+    long double c, s;
+    tara::twiddle(m, Nx, c, s);
+    t.tw_real[m] = tara::cx<double>((double)c, (double)s);
+  }
+  for (int i = 0; i < Nh; i++) t.kx[i] = 2.0 * p->pi * (double)i / p->Lx;
+  for (int j = 0; j < Ny; j++)
+    t.ky[j] = (j < Ny / 2) ? 2.0 * p->pi * (double)j / p->Ly : 2.0 * p->pi * (double)(j - Ny) / p->Ly;
+  const double thr = ((double)(Nx + Ny) / 2.0) / 3.0 + 0;
+  for (int j = 0; j < Ny; j++) {
+    int c = Nh;
+    for (int i = 0; i < Nh; i++) {
+      volatile double a = t.kx[i] * t.kx[i];
+      volatile double b = t.ky[j] * t.ky[j];
+      volatile double sum = a + b;
+      if (std::sqrt((double)sum) >= thr) { c = i; break; }
+    }
+    t.cut[j] = c;
+  }
+  g_key_n[0] = Nx;
+  g_key_n[1] = Ny;
+  g_key_d[0] = p->Lx;
+  g_key_d[1] = p->Ly;
+  g_key_d[2] = p->pi;
+}
+
+// Device address of the workspace on the current device.  Called with g_mu held.
+int scratch_address(int dev, void** out) {
   if (dev < 0 || dev >= kMaxDevices) {
     tara::set_error("device index out of range for the static workspace table");
     return TARA_EINVAL;
   }
   if (!g_scratch_addr[dev]) {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess || !p) {
       tara::set_error(std::string("cudaGetSymbolAddress(workspace): ") + cudaGetErrorString(e));
       return TARA_ECUDA;
@@ -93,75 +183,48 @@ extern "C" int tara_derive2coh_noalloc(const tara_params* p, int Nx, int Ny, con
     set_error("tara_derive2coh_noalloc: Nx and Ny must be one of 16, 32, 64, 128, 256 (static workspace limit)");
     return TARA_EINVAL;
   }
-  void* base = nullptr;
-  int r = scratch_address(&base);
-  if (r != TARA_OK) return r;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int Nh = Nx / 2 + 1, M = Nx / 2;
-
-  // Tables, built on the host into fixed buffers with the reference formulas
-  // (kx, ky: src/derive2coh.f95:58-86; 2/3 rule: :208-212).
-  for (int m = 0; m < Ny; m++) { long double c, s; twiddle(m, Ny, c, s); h_tw_col[m] = cx<double>((double)c, (double)s); }
-  for (int m = 0; m < M; m++) { long double c, s; twiddle(m, M, c, s); h_tw_row[m] = cx<double>((double)c, (double)s); }
-  for (int m = 0; m <= M; m++) { long double c, s; twiddle(m, Nx, c, s); h_tw_real[m] = cx<double>((double)c, (double)s); }
-  for (int i = 0; i < Nh; i++) h_kx[i] = 2.0 * p->pi * (double)i / p->Lx;
-  for (int j = 0; j < Ny; j++)
-    h_ky[j] = (j < Ny / 2) ? 2.0 * p->pi * (double)j / p->Ly : 2.0 * p->pi * (double)(j - Ny) / p->Ly;
-  const double thr = ((double)(Nx + Ny) / 2.0) / 3.0 + 0;
-  for (int j = 0; j < Ny; j++) {
-    int c = Nh;
-    for (int i = 0; i < Nh; i++) {
-      volatile double a = h_kx[i] * h_kx[i];
-      volatile double b = h_ky[j] * h_ky[j];
-      volatile double sum = a + b;
-      if (std::sqrt((double)sum) >= thr) { c = i; break; }
-    }
-    h_cut[j] = c;
-  }
-  size_t off[6], o = 0;
-  const size_t bytes[6] = {Ny * sizeof(Cx<double>), M * sizeof(Cx<double>), (M + 1) * sizeof(Cx<double>),
-                           Nh * sizeof(double), Ny * sizeof(double), Ny * sizeof(int)};
-  const void* src[6] = {h_tw_col, h_tw_row, h_tw_real, h_kx, h_ky, h_cut};
-  for (int q = 0; q < 6; q++) {
-    off[q] = o;
-    std::memcpy(h_tables + o, src[q], bytes[q]);
-    o += (bytes[q] + 255) / 256 * 256;
-  }
-  unsigned char* dtab = static_cast<unsigned char*>(base) + 11 * kField * sizeof(Cx<double>);
-  cudaError_t e = cudaMemcpyAsync(dtab, h_tables, o, cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) {
-    set_error(std::string("tara_derive2coh_noalloc: table upload: ") + cudaGetErrorString(e));
-    return TARA_ECUDA;
-  }
-
-  Grid<double> g;  // describes the static workspace; init()/release() are never called
-  g.Nx = Nx; g.Ny = Ny; g.Nh = Nh; g.ld = Nh;
-  g.Lx = p->Lx; g.Ly = p->Ly; g.pi = p->pi;
-  g.tb.tw_col = reinterpret_cast<const Cx<double>*>(dtab + off[0]);
-  g.tb.tw_row = reinterpret_cast<const Cx<double>*>(dtab + off[1]);
-  g.tb.tw_real = reinterpret_cast<const Cx<double>*>(dtab + off[2]);
-  g.tb.kx = reinterpret_cast<const double*>(dtab + off[3]);
-  g.tb.ky = reinterpret_cast<const double*>(dtab + off[4]);
-  g.tb.cut = reinterpret_cast<const int*>(dtab + off[5]);
-  g.tb.Nx = Nx; g.tb.Ny = Ny; g.tb.Nh = Nh; g.tb.ld = Nh;
-  const double nn = (double)Nx * (double)Ny;
-  g.tb.nn = nn;
-  g.tb.inv_nn = 1.0 / nn;
-  g.tb.nn_pow2 = 1;  // every accepted size is a power of two
-  // status word of the kernels' bounded waits: the last 256 bytes of the table region
-  g.tb.status = reinterpret_cast<int*>(dtab + kTableBytes - 256);
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
     set_error("tara_derive2coh_noalloc: device query failed");
     return TARA_ECUDA;
   }
-  g.tb.sm_count = sms;
-  const int zero = 0;
-  e = cudaMemcpyAsync(g.tb.status, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) {
-    set_error(std::string("tara_derive2coh_noalloc: status reset: ") + cudaGetErrorString(e));
-    return TARA_ECUDA;
+  void* base = nullptr;
+  unsigned char* dtab = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    const int r = scratch_address(dev, &base);
+    if (r != TARA_OK) return r;
+    build_tables(Nx, Ny, p);
+    dtab = static_cast<unsigned char*>(base) + 11 * kField * sizeof(Cx<double>);
+    // the launch copies g_tab into its parameters, so the lock may end after it
+    k_noalloc_tables<<<1, 256, 0, st>>>(g_tab, dtab, Ny, M, Nh);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      set_error(std::string("tara_derive2coh_noalloc: table upload: ") + cudaGetErrorString(e));
+      return TARA_ECUDA;
+    }
   }
+
+  Grid<double> g;  // describes the static workspace; init()/release() are never called
+  g.Nx = Nx; g.Ny = Ny; g.Nh = Nh; g.ld = Nh;
+  g.Lx = p->Lx; g.Ly = p->Ly; g.pi = p->pi;
+  g.tb.tw_col = reinterpret_cast<const Cx<double>*>(dtab + kOffTwCol);
+  g.tb.tw_row = reinterpret_cast<const Cx<double>*>(dtab + kOffTwRow);
+  g.tb.tw_real = reinterpret_cast<const Cx<double>*>(dtab + kOffTwReal);
+  g.tb.kx = reinterpret_cast<const double*>(dtab + kOffKx);
+  g.tb.ky = reinterpret_cast<const double*>(dtab + kOffKy);
+  g.tb.cut = reinterpret_cast<const int*>(dtab + kOffCut);
+  g.tb.Nx = Nx; g.tb.Ny = Ny; g.tb.Nh = Nh; g.tb.ld = Nh;
+  const double nn = (double)Nx * (double)Ny;
+  g.tb.nn = nn;
+  g.tb.inv_nn = 1.0 / nn;
+  g.tb.nn_pow2 = 1;  // every accepted size is a power of two
+  g.tb.status = reinterpret_cast<int*>(dtab + kOffStatus);  // written by no kernel of this path
+  g.tb.sm_count = sms;
+  g.tb.no_tma = 1;  // register-staged column passes: no TMA loads, no bounded waits
+  g.tb.wait_ns = 0;
 
   // fields of this grid packed back to back in the workspace
   const size_t fe = (size_t)Ny * Nh;

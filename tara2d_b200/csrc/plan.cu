@@ -134,6 +134,8 @@ int Grid<T>::init(int nx, int ny, double lx, double ly, double pi_, cudaStream_t
   TARA_CUDA_TRY(cudaGetDevice(&dev));
   TARA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   tb.sm_count = sms;
+  tb.no_tma = 0;
+  tb.wait_ns = 1000000000ull;
   tb.Nx = nx; tb.Ny = ny; tb.Nh = Nh; tb.ld = ld;
   double nn = (double)nx * (double)ny;
   tb.nn = (T)nn;

@@ -17,6 +17,7 @@ enum KernelKind : int {
   KK_ROW_VORT,
   KK_COL_FWD_VORT,
   KK_ROW_FORCE,
+  KK_CFL,
   KK_END,  // marks the end of the previous kernel
   KK_COUNT
 };
@@ -24,7 +25,7 @@ enum KernelKind : int {
 inline const char* kernel_kind_name(int k) {
   static const char* n[KK_COUNT] = {"k_col_inv",      "k_row_coh",   "k_col_fwd_simple", "k_row_com1",
                                     "k_col_rt",       "k_row_com2",  "k_col_fwd_com",    "k_row_vort",
-                                    "k_col_fwd_vort", "k_row_force", "end"};
+                                    "k_col_fwd_vort", "k_row_force", "k_cfl_update", "end"};
   return (k >= 0 && k < KK_COUNT) ? n[k] : "?";
 }
 

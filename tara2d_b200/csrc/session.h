@@ -62,4 +62,9 @@ struct tara_session {
   // the state was changed from outside the stepping kernels: drop what was
   // derived from it
   virtual void invalidate_derived() = 0;
+  // CFL control (TARA_CFL_*), model time, bounded-wait limit
+  virtual int set_cfl(int mode, double number) = 0;
+  virtual int get_time(double* t, double* dt) = 0;
+  virtual int set_time(double t) = 0;
+  virtual int set_wait_limit(long long ns) = 0;
 };

@@ -35,6 +35,8 @@ struct Tables {
   int nn_pow2;           // Nx*Ny is a power of two (so x*inv_nn == x/nn exactly)
   int* status;           // device status word (TARA_ETIMEOUT after a bounded wait ran out)
   int sm_count;          // multiprocessors of the device (persistent grids)
+  int no_tma;            // 1: column passes use the register-staged kernels (no TMA, no bounded waits)
+  unsigned long long wait_ns;  // limit of every bounded wait of the TMA kernels, in ns of %globaltimer
 };
 
 template <class T> __device__ __forceinline__ Cx<T> ldg(const Cx<T>* p);

@@ -6,8 +6,9 @@
 // {2*CB, BOX}; its x coordinate 2*c0 is always a multiple of 16 bytes.  The
 // box lands in shared memory row-major: element (t, i) of the tile at
 // i*CB + t.  Completion is tracked by an mbarrier with a transaction count.
-// Every wait is bounded (about one second of %globaltimer); a kernel whose
-// wait runs out records TARA_ETIMEOUT in the grid's status word and stops.
+// Every wait is bounded (Tables::wait_ns of %globaltimer, one second unless
+// the session sets another limit); a kernel whose wait runs out records
+// TARA_ETIMEOUT in the grid's status word and stops.
 #pragma once
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -66,13 +67,15 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
 }
-// Waits for phase `parity` of the barrier for at most ~1 s; false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+// Waits for phase `parity` of the barrier for at most limit_ns nanoseconds of
+// %globaltimer (the kernels take the limit from Tables::wait_ns, one second
+// by default); false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (global_ns() - t0 > 1000000000ull) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
 }
 // Orders this thread's earlier generic-proxy shared-memory accesses before
