@@ -350,6 +350,50 @@ def run_mhd3d(args):
     return 0
 
 
+# ------------------------------------------------------------------ 4096^2 FP32
+def run_mhd4096(args):
+    """Side line (not the headline): the large single-GPU configuration, 2D
+    MHD at 4096^2, RK4, FP32 fields and FFTs with FP64 reductions, nu = eta =
+    2e-5, random-phase u and B with E(k) ~ k^4 exp(-(k/6)^2) (seed 11),
+    dt = 1.5e-5 (under the acoustic CFL limit), --steps steps (500 by the
+    configuration).  Its error against the FP64 oracle over the first 50
+    steps is checked by tests/test_fullrun_gpu.py."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import tara2d_b200 as T
+    from tara2d_b200 import initial
+    n = 4096
+    T.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    kw = dict(params_dict(), mu=2e-5, eta=2e-5, dt=1.5e-5)
+    W, K = max(3, args.warmup), max(1, args.steps)
+    peak, peak_kind = peaks()
+    with T.Session(T.MODEL_COM, n, n, T.Params.make(**kw), precision=T.FP32) as s:
+        s.set_state(initial.com_random_phase(n, n, seed=11, k0=6.0))
+        s.step(T.STEP_RK4, W)
+        clk = ClockSampler(T.device_pci_bus_id())
+        clk.start()
+        ms = s.time_steps(T.STEP_RK4, K)
+        clocks = clk.stop()
+        launches = s.launches_per_step(T.STEP_RK4)
+    S = n * ((n // 2 + 1 + 15) // 16 * 16) * 8  # FP32 spectral field with its row pitch
+    S_alg = n * (n // 2 + 1) * 8
+    bps = 4 * (4 * 17 + 4 * 6) * S_alg
+    per_s = K / (ms / 1e3)
+    out = {"metric": "MHD RK4 steps/s at 4096^2, FP32 bulk with FP64 reductions", "value": per_s,
+           "unit": "steps/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "2D compressible MHD (*2com), 4096x4096, FP32, RK4 dt=1.5e-5, nu=eta=2e-5, "
+                                  "CS=100, random-phase u and B, E(k)~k^4 exp(-(k/6)^2) (seed 11)",
+                      "l2": f"working set {42 * S / 1e9:.1f} GB > 126 MB L2; no flush"},
+           "grid_point_steps_per_s": per_s * n * n,
+           "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": bps * per_s / 1e9, "peak": peak,
+                        "unit": "GB/s", "frac": bps * per_s / 1e9 / peak, "bytes_per_step": bps,
+                        "peak_source": peak_kind, "note": "n_RHS (4T+4F) S per RK4 step, T=17, F=6, S FP32"},
+           "clocks": clocks, "gpu_launches": launches * K}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ per-kernel table
 def kernel_table_bytes(model: str, rk4: bool, S: float) -> dict:
     """Algorithmic bytes of one launch of each kernel of a model's RHS (every
@@ -414,6 +458,57 @@ def run_kernels(args):
     return 0
 
 
+# ------------------------------------------------------------------ FFT engine vs cuFFT
+def run_fft(args):
+    """Timed comparison (not the headline): the engine's plain 2D c2r and
+    r2c (the transforms that replace the reference's dfftw_execute of its
+    r2c / c2r plans, src/derive2com.f95:70-248) against cuFFT (through
+    torch.fft, outside the library) on the same sizes, layout and data, FP64,
+    1 and 6 fields per call.  CUDA events on each side's own stream, median of
+    5 runs of --steps calls each after warm-up."""
+    import torch
+    import tara2d_b200 as T
+    T.set_device(0)
+    peak, peak_kind = peaks()
+    reps = max(5, args.steps)
+    rows = []
+    for n in (1024, 4096):
+        with T.Session(T.MODEL_COM, n, n, T.Params.make(**params_dict())) as s:
+            s.set_state_random(T.IC_RANDOM_PHASE, 3, k0=6.0, e1=0.5, e2=0.5)
+            spec = [torch.from_numpy(a).to("cuda:0") for a in s.get_state()]
+            for inverse in (1, 0):
+                for nf in (1, 6):
+                    s.time_transforms(inverse, nf, 3)
+                    ours = statistics.median(s.time_transforms(inverse, nf, reps) / reps for _ in range(5))
+                    X = torch.stack(spec[:nf])
+                    R = torch.fft.irfft2(X, s=(n, n), norm="forward")
+                    fn = (lambda: torch.fft.irfft2(X, s=(n, n), norm="forward")) if inverse else \
+                        (lambda: torch.fft.rfft2(R, norm="backward"))
+                    for _ in range(3):
+                        fn()
+                    times = []
+                    for _ in range(5):
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        torch.cuda.synchronize()
+                        e0.record()
+                        for _ in range(reps):
+                            fn()
+                        e1.record()
+                        e1.synchronize()
+                        times.append(e0.elapsed_time(e1) / reps)
+                    cu = statistics.median(times)
+                    byts = nf * (n * (n // 2 + 1) * 16 + n * n * 8)  # spectral in/out + real out/in, once
+                    rows.append({"N": n, "direction": "c2r" if inverse else "r2c", "fields": nf,
+                                 "ours_us_per_field": ours * 1e3 / nf, "cufft_us_per_field": cu * 1e3 / nf,
+                                 "ours_GBps": byts / (ours / 1e3) / 1e9, "cufft_GBps": byts / (cu / 1e3) / 1e9,
+                                 "ours_frac": byts / (ours / 1e3) / 1e9 / peak,
+                                 "cufft_frac": byts / (cu / 1e3) / 1e9 / peak, "cufft_over_ours": cu / ours})
+    print(json.dumps({"workload": "fft", "metric": "2D FP64 transform time per field, ours vs cuFFT",
+                      "unit": "us", "peak_GBps": peak, "peak_source": peak_kind, "reps": reps, "rows": rows}),
+          flush=True)
+    return 0
+
+
 # ------------------------------------------------------------------ ranks
 class Ranks:
     """One process per GPU (replicas: the path does not shard).  Rank and
@@ -472,9 +567,10 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=1024, help="grid size (profiling runs only; the metric is at 1024)")
-    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "mhd3d", "kernels"],
+    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "mhd3d", "kernels", "fft", "mhd4096"],
                     help="mhd1024: the headline; ensemble: the 256-run batched side workload; "
-                         "mhd3d: the 3D path at --grid3^3; kernels: per-kernel times of --model at --grid")
+                         "mhd3d: the 3D path at --grid3^3; kernels: per-kernel times of --model at --grid; "
+                         "fft: the engine's 2D transforms against cuFFT; mhd4096: 4096^2 FP32 MHD")
     ap.add_argument("--grid3", type=int, default=256, help="3D grid size of --workload mhd3d")
     ap.add_argument("--model", choices=["com", "coh", "csh", "css"], default="com", help="--workload kernels")
     ap.add_argument("--fp32", action="store_true", help="--workload kernels: FP32 session")
@@ -490,6 +586,10 @@ def main():
         return run_mhd3d(args)
     if args.workload == "kernels":
         return run_kernels(args)
+    if args.workload == "fft":
+        return run_fft(args)
+    if args.workload == "mhd4096":
+        return run_mhd4096(args)
 
     ranks = Ranks("nccl")
     world, rank, local = ranks.world, ranks.rank, ranks.local

@@ -96,6 +96,14 @@ int tara_synchronize(tara_session* s);
 int tara_time_steps(tara_session* s, int stepper, int nsteps, float* ms);
 /* Kernel launches one step of the given stepper issues. */
 int tara_launches_per_step(const tara_session* s, int stepper);
+/* Device time of reps plain 2D transforms of nfields fields (1 .. min(6,
+ * fields of the model)) on device-resident buffers, the transforms that
+ * replace FFTW's dfftw_execute of an r2c / c2r plan (src/derive2com.f95:70-248):
+ * inverse = 1: c2r of the state fields into real fields (normalised by
+ * Nx Ny, as the drivers divide after every c2r); inverse = 0: r2c of those
+ * real fields into work fields (the state is left as it is).  CUDA events on
+ * the session stream; *ms is the total of the reps. */
+int tara_time_transforms(tara_session* s, int inverse, int nfields, int reps, float* ms);
 /* Steps are replayed from CUDA graphs of two steps each (captured on first
  * use per stepper, dropped on tara_set_params); on = 0 launches every kernel
  * from the host instead.  Default: on. */

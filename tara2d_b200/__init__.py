@@ -157,6 +157,7 @@ def lib():
         L.tara_get_time.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.tara_set_time.argtypes = [P, D]
         L.tara_set_wait_limit.argtypes = [P, C.c_longlong]
+        L.tara_time_transforms.argtypes = [P, I, I, I, C.POINTER(C.c_float)]
         L.tara_selftest_bounded_wait.argtypes = [C.c_longlong, C.POINTER(C.c_longlong)]
         _lib = L
     return _lib
@@ -338,6 +339,12 @@ class Session:
 
     def set_time(self, t: float) -> None:
         check(lib().tara_set_time(self._h, t), "tara_set_time")
+
+    def time_transforms(self, inverse: int, nfields: int, reps: int) -> float:
+        """Device ms of reps plain 2D c2r (inverse = 1) or r2c of nfields fields."""
+        ms = C.c_float()
+        check(lib().tara_time_transforms(self._h, inverse, nfields, reps, C.byref(ms)), "tara_time_transforms")
+        return ms.value
 
     def set_wait_limit(self, ns: int) -> None:
         check(lib().tara_set_wait_limit(self._h, int(ns)), "tara_set_wait_limit")

@@ -713,6 +713,41 @@ struct SessionT : tara_session {
     return r == TARA_OK ? device_status() : r;
   }
 
+  int time_transforms(int inverse, int nfields, int reps, float* ms) override {
+    if (nfields < 1 || nfields > nf || nfields > 6 || reps < 1 || !ms) {
+      set_error("bad transform timing request");
+      return TARA_EINVAL;
+    }
+    TARA_TRY(ensure_real());
+    h_for = nullptr;  // the transforms use the work pool
+    if (workpool().count < nfields) { set_error("work pool too small"); return TARA_EINVAL; }
+    const size_t nn = (size_t)Nx * Ny;
+    T* r[6];
+    const T* rc[6];
+    const Cx<T>* uc[6];
+    Cx<T>* sp[6];
+    Cx<T>* wk[6];
+    for (int q = 0; q < nfields; q++) {
+      r[q] = rbuf + q * nn;
+      rc[q] = r[q];
+      uc[q] = u[q];
+      sp[q] = tmp[q];
+      wk[q] = workpool()[q];
+    }
+    // real fields to transform forward: the state's own c2r
+    if (!inverse) TARA_TRY(c2r_fields<T>(g, nfields, uc, r, wk, true, st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
+    TARA_CUDA_TRY(cudaEventRecord(ev0, st));
+    for (int k = 0; k < reps; k++) {
+      if (inverse) TARA_TRY(c2r_fields<T>(g, nfields, uc, r, wk, true, st));
+      else TARA_TRY(r2c_fields<T>(g, nfields, rc, sp, wk, st));
+    }
+    TARA_CUDA_TRY(cudaEventRecord(ev1, st));
+    TARA_CUDA_TRY(cudaEventSynchronize(ev1));
+    TARA_CUDA_TRY(cudaEventElapsedTime(ms, ev0, ev1));
+    return device_status();
+  }
+
   int num_shells() override { return diag_num_shells(Nx, Ny, p.Lx, p.Ly, p.pi); }
   int record(double* drec) {
     h_for = nullptr;  // the diagnostics use the work pool
@@ -928,6 +963,9 @@ int tara_device_pci_bus_id(char* out, int len) {
 }
 
 int tara_launches_per_step(const tara_session* s, int stepper) { return s ? s->launches(stepper) : 0; }
+int tara_time_transforms(tara_session* s, int inverse, int nfields, int reps, float* ms) {
+  return s ? s->fail_if(s->time_transforms(inverse, nfields, reps, ms)) : TARA_EINVAL;
+}
 
 int tara_get_state_real(tara_session* s, double* const* fields) {
   return s ? s->fail_if(s->real_fields(0, fields)) : TARA_EINVAL;

@@ -54,6 +54,8 @@ struct tara_session {
   // after every `every` steps (nsteps = (nrec - 1) * every), into rec
   // (host, nrec * (TARA_DIAG_VALUES + num_shells()) doubles)
   virtual int run_recorded(int stepper, int every, int nrec, double* rec) = 0;
+  // device time of reps plain 2D c2r (inverse) or r2c of nfields fields
+  virtual int time_transforms(int inverse, int nfields, int reps, float* ms) = 0;
   // for the closure code: the grid (const tara::Grid<T>*), state field q
   // (tara::Cx<T>*), and the closure whose term the MHD RHS adds (NULL: none)
   virtual const void* grid_ptr() const = 0;

@@ -83,7 +83,6 @@ def _check_com_diag(vals, eks, fx, rtol, rtol_w2=None, ek_tol=None):
     return rel.max(axis=0)
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(GOLD, "run_com1024_rk4.npz")), reason="fixture not generated")
 def test_config2_mhd_1024_rk4_2000_steps(tara):
     """1024^2 MHD (perturbed Orszag-Tang), RK4, dt = 5e-5, nu = eta = 5e-4,
     2000 steps, diagnostics every 100 (the Energy.dat cadence of
@@ -100,7 +99,6 @@ def test_config2_mhd_1024_rk4_2000_steps(tara):
     assert rel_fields(low_modes(states[1]), fx["fields_low"][1]) <= 1e-8
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(GOLD, "run_com4096_rk4.npz")), reason="fixture not generated")
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_config5_mhd_4096_rk4_first_50_steps_vs_fp64_oracle(tara, prec):
     """4096^2 MHD, nu = eta = 2e-5, E(k) ~ k^4 exp(-(k/6)^2), dt = 1.5e-5

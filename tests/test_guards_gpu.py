@@ -20,6 +20,7 @@ import numpy as np
 import pytest
 
 from tests.gpu_common import PI, coh_kw, com_kw, oracle_coh_params, oracle_com_params, rel_l2
+from tests.test_parity_com_gpu import compressive
 from tara2d_b200 import initial as I
 
 pytestmark = pytest.mark.gpu
@@ -77,7 +78,7 @@ def test_cfl_adaptive_rk4_run_com(tara, oracle):
     configured dt, against the oracle stepped with the dt sequence the rate
     of its own state gives."""
     N, C, nsteps = 64, 0.8, 20
-    kw = com_kw(dt=2e-3, CS=10.0)
+    kw = com_kw(dt=1e-2, CS=10.0)  # dt_cfl is about 3.6e-3 here
     st0 = I.com_random_phase(N, N, seed=23, CS=10.0)
     with tara.Session(tara.MODEL_COM, N, N, tara.Params.make(**kw)) as s:
         s.set_state(st0)
@@ -208,10 +209,11 @@ def test_bounded_wait_runs_out(tara, oracle):
     st, waited = tara.selftest_bounded_wait(1_000_000)  # 1 ms
     assert st == tara.ETIMEOUT, (st, tara.last_error())
     assert 1_000_000 <= waited < 1_000_000_000, waited
-    # the context is still usable: a RHS against the oracle
+    # the context is still usable: a RHS against the oracle (compressive
+    # noise, so that d(rho)/dt is not rounding noise)
     N = 64
     kw = com_kw()
-    s0 = I.com_random_phase(N, N, seed=8)
+    s0 = compressive(I.com_random_phase(N, N, seed=8), 8)
     with tara.Session(tara.MODEL_COM, N, N, tara.Params.make(**kw)) as s:
         s.set_wait_limit(2_000_000_000)
         s.set_state(s0)
