@@ -277,25 +277,37 @@ int tara_filter_state(tara_session* fine, tara_session* coarse);
 
 /* ---- batched ensembles (no counterpart in the reference, whose drivers run
  * one grid per process) ----
- * n independent hydro (*2coh) runs, member m on an N[m] x N[m] grid
- * (N in {128, 256, 384, 512}) with its own parameters params[m] (mux, muy,
- * CS, dt; members of one grid size share Lx, Ly, pi), advanced together: each
- * step is three persistent launches over every member (column inverse, row
- * pass, column forward with the AB2/Euler update), replayed from a CUDA graph.
- * State arrays are complex(8) (Nh,Ny) host arrays as for sessions; AB2
- * history starts at zero.  FP32 or FP64 fields; diagnostics sum in FP64. */
+ * n independent runs, member m a hydro (*2coh, src/derive2coh.f95) or MHD
+ * (*2com, src/derive2com.f95) run on an N[m] x N[m] grid (N in {128, 256,
+ * 384, 512}) with its own parameters params[m] (hydro: mux, muy, CS, dt; MHD:
+ * mu, eta, CS, dt with A = 0 and fix_curlB = 0; members of one grid size
+ * share Lx, Ly, pi), advanced together: each step is three persistent
+ * launches over every hydro member (column inverse, row pass, column forward
+ * with the AB2/Euler update) and four over every MHD member (first row pass,
+ * d(uy)/dy, second row pass, column forward with the update and the y-inverse
+ * of the new state; a column inverse first where the state was just set),
+ * replayed from a CUDA graph.  Each member is bit-identical to a session run
+ * of it.  State arrays are complex(8) (Nh,Ny) host arrays as for sessions,
+ * tara_ens_num_fields(e, m) of them (3 hydro, 6 MHD); AB2 history starts at
+ * zero.  FP32 or FP64 fields; diagnostics sum in FP64. */
 typedef struct tara_ensemble tara_ensemble;
+/* every member runs `model` (TARA_MODEL_COH or TARA_MODEL_COM) */
 int tara_ens_open(tara_ensemble** out, int model, int n, const int* N, const tara_params* params, int precision);
+/* member m runs models[m] */
+int tara_ens_open_mixed(tara_ensemble** out, int n, const int* models, const int* N, const tara_params* params,
+                        int precision);
 int tara_ens_close(tara_ensemble* e);
 int tara_ens_size(const tara_ensemble* e);
-int tara_ens_set_state(tara_ensemble* e, int member, const double* const* fields3);
-int tara_ens_get_state(tara_ensemble* e, int member, double* const* fields3);
-int tara_ens_get_history(tara_ensemble* e, int member, double* const* fields3);
+int tara_ens_num_fields(const tara_ensemble* e, int member);
+int tara_ens_set_state(tara_ensemble* e, int member, const double* const* fields);
+int tara_ens_get_state(tara_ensemble* e, int member, double* const* fields);
+int tara_ens_get_history(tara_ensemble* e, int member, double* const* fields);
 int tara_ens_step(tara_ensemble* e, int stepper, int nsteps); /* TARA_STEP_AB2 or TARA_STEP_EULER */
 int tara_ens_time_steps(tara_ensemble* e, int stepper, int nsteps, float* ms);
-/* Tuning: {values per thread of the column inverse, the row pass and the
- * column forward pass (8 or 16), CTAs per SM of each persistent grid (0 = as
- * many as fit)}.  Default {16, 16, 16, 0, 0, 0}. */
+/* Tuning of the hydro phases: {values per thread of the column inverse, the
+ * row pass and the column forward pass (8 or 16), CTAs per SM of each
+ * persistent grid (0 = as many as fit)}.  Default {16, 16, 16, 0, 0, 0}.
+ * The MHD phases keep the sessions' values per thread. */
 int tara_ens_set_tuning(tara_ensemble* e, const int* tuning6);
 int tara_ens_get_tuning(const tara_ensemble* e, int* tuning6);
 /* Times every candidate per phase on this ensemble (reps steps each, state

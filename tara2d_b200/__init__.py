@@ -130,6 +130,8 @@ def lib():
         L.tara_checkpoint_read.argtypes = [P, C.c_char_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
         L.tara_format_list_directed.argtypes = [P, I, C.c_char_p, I]
         L.tara_ens_open.argtypes = [C.POINTER(C.c_void_p), I, I, P, C.POINTER(Params), I]
+        L.tara_ens_open_mixed.argtypes = [C.POINTER(C.c_void_p), I, P, P, C.POINTER(Params), I]
+        L.tara_ens_num_fields.argtypes = [P, I]
         L.tara_ens_close.argtypes = [P]
         for n in ("tara_ens_set_state", "tara_ens_get_state", "tara_ens_get_history"):
             getattr(L, n).argtypes = [P, I, PP]
@@ -642,11 +644,13 @@ def format_list_directed(values) -> str:
 
 
 class Ensemble:
-    """Independent hydro runs of mixed grid sizes advanced together
-    (tara_ens_open ... tara_ens_close).  sizes[m] in {128, 256, 384, 512};
-    params[m] is a Params (or one Params for every member)."""
+    """Independent hydro and/or MHD runs of mixed grid sizes advanced together
+    (tara_ens_open / tara_ens_open_mixed ... tara_ens_close).  sizes[m] in
+    {128, 256, 384, 512}; params[m] is a Params (or one Params for every
+    member); model is MODEL_COH or MODEL_COM for every member, or a list with
+    one model per member."""
 
-    def __init__(self, sizes, params, precision: int = FP32, model: int = MODEL_COH):
+    def __init__(self, sizes, params, precision: int = FP32, model=MODEL_COH):
         self.sizes = [int(n) for n in sizes]
         n = len(self.sizes)
         if isinstance(params, Params):
@@ -655,7 +659,14 @@ class Ensemble:
         arr = (Params * n)(*self.params)
         ns = (C.c_int * n)(*self.sizes)
         h = C.c_void_p()
-        check(lib().tara_ens_open(C.byref(h), model, n, ns, arr, precision), "tara_ens_open")
+        if isinstance(model, (list, tuple)):
+            self.models = [int(x) for x in model]
+            assert len(self.models) == n
+            ms = (C.c_int * n)(*self.models)
+            check(lib().tara_ens_open_mixed(C.byref(h), n, ms, ns, arr, precision), "tara_ens_open_mixed")
+        else:
+            self.models = [int(model)] * n
+            check(lib().tara_ens_open(C.byref(h), int(model), n, ns, arr, precision), "tara_ens_open")
         self._h = h
 
     def close(self) -> None:
@@ -682,12 +693,15 @@ class Ensemble:
         if not 0 <= m < len(self.sizes):
             raise TaraError(f"no ensemble member {m}")
         N = self.sizes[m]
-        return [np.zeros((N, N // 2 + 1), dtype=np.complex128) for _ in range(3)]
+        nf = lib().tara_ens_num_fields(self._h, m)
+        return [np.zeros((N, N // 2 + 1), dtype=np.complex128) for _ in range(nf)]
 
     def set_state(self, m: int, fields) -> None:
         N = self.sizes[m]
         a = [np.ascontiguousarray(f, dtype=np.complex128) for f in fields]
-        assert len(a) == 3 and all(x.shape == (N, N // 2 + 1) for x in a)
+        nf = lib().tara_ens_num_fields(self._h, m)
+        if len(a) != nf or not all(x.shape == (N, N // 2 + 1) for x in a):
+            raise TaraError(f"member {m} takes {nf} fields of shape {(N, N // 2 + 1)}")
         check(lib().tara_ens_set_state(self._h, m, _ptrs(a)), "tara_ens_set_state")
 
     def get_state(self, m: int):

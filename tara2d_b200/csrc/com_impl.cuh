@@ -59,8 +59,10 @@ template <class T> struct RowCom1Args {
   CflRow cfl;  // cfl.lam set: fold the rows' largest signal-speed rate into it
 };
 
+// Rows y0 .. y0 + (blockDim.x / (8 M/P)) - 1 by the whole CTA (8 groups of
+// M/P threads per row), in the CTA's dynamic shared memory.
 template <class T, int M, int P, bool LOW>
-__global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const RowCom1Args<T> a) {
+__device__ __forceinline__ void row_com1_rows(const RowCom1Args<T>& a, int y0) {
   using RF = RowFFT<M, P>;
   constexpr int NTR = M / P, G = 8, ARR = RF::SMEM_ELEMS, NA = LOW ? 6 : 8;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
   Cx<T>* f[8];  // rho, rho ux, rho uy, E, Bx, By, ux, uy (pairs x[2m], x[2m+1])
 #pragma unroll
   for (int q = 0; q < 8; q++) f[q] = base + (q < NA ? q : q - NA) * ARR;
-  const int y = blockIdx.x * a.rb + th.row;
+  const int y = y0 + th.row;
   const size_t ro = (size_t)y * tb.ld;
   Cx<T> v[P];
   // phase 1: six c2r along x, normalised         (src/derive2com.f95:70-102)
@@ -167,6 +169,10 @@ __global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const Row
     if (q >= NA) row_r2c_finish<RF>(f[q], th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
   }
 }
+template <class T, int M, int P, bool LOW>
+__global__ void __launch_bounds__(TARA_ROW_LB(8 * (M / P))) k_row_com1(const RowCom1Args<T> a) {
+  row_com1_rows<T, M, P, LOW>(a, blockIdx.x * a.rb);
+}
 
 // Forcing (only when A != 0):  Fx = -rho A sin(kf y_j), Fy = rho A sin(kf x_i)
 // on the grid x_i = (i-1) dx, y_j = (j-1) dy                       (:109-110)
@@ -223,10 +229,9 @@ template <class T> struct RowCom2Args {
   int rb;
 };
 
+// Rows y0 .. by the whole CTA (G groups of M/P threads per row).
 template <class T, int M, int P, int FIX>
-__global__ void __launch_bounds__(TARA_ROW_LB((FIX ? 6 : 4) * (M / P)),
-                                  TARA_MINB(TARA_ROW_LB((FIX ? 6 : 4) * (M / P))))
-k_row_com2(const RowCom2Args<T> a) {
+__device__ __forceinline__ void row_com2_rows(const RowCom2Args<T>& a, int y0) {
   using RF = RowFFT<M, P>;
   constexpr int NTR = M / P, G = FIX ? 6 : 4, NA = FIX ? 6 : 5, ARR = RF::SMEM_ELEMS;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -240,7 +245,7 @@ k_row_com2(const RowCom2Args<T> a) {
   Cx<T>* by = base + 3 * ARR;
   Cx<T>* curl = base + 4 * ARR;
   Cx<T>* aux = base + (NA - 1) * ARR;  // dBx/dy when corrected
-  const int y = blockIdx.x * a.rb + th.row;
+  const int y = y0 + th.row;
   const size_t ro = (size_t)y * tb.ld;
   const T* kx = tb.kx;
   Cx<T> v[P];
@@ -303,6 +308,12 @@ k_row_com2(const RowCom2Args<T> a) {
     row_r2c_finish<RF>(base + g * ARR, th.lane, NTR, v, tb, [&](int k, Cx<T> X) { st(xo + k, X); }, sync);
   }
 }
+template <class T, int M, int P, int FIX>
+__global__ void __launch_bounds__(TARA_ROW_LB((FIX ? 6 : 4) * (M / P)),
+                                  TARA_MINB(TARA_ROW_LB((FIX ? 6 : 4) * (M / P))))
+k_row_com2(const RowCom2Args<T> a) {
+  row_com2_rows<T, M, P, FIX>(a, blockIdx.x * a.rb);
+}
 
 
 template <class T> struct ColFwdComArgs {
@@ -329,126 +340,18 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_c
   Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
   const int f = blockIdx.y;
   const int c0 = blockIdx.x * CB;
-  const int Nh = a.tb.Nh, ld = a.tb.ld;
-  const T* kx = a.tb.kx;
-  const T* ky = a.tb.ky;
-  const int tid = threadIdx.x;
-  Cx<T> v[P], d[P];
-  // forward transform of X (+ X2: two parts of one flux, summed as loaded)
-  auto fft = [&](const Cx<T>* X, const Cx<T>* X2 = nullptr) {
-    __syncthreads();
-    fft_run<F, -1>(sm, tid, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
-      const int c = c0 + t;
-      if (c >= Nh) return cx<T>(0, 0);
-      const size_t o = (size_t)i * ld + c;
-      return X2 ? ldg(X + o) + ldg(X2 + o) : ldg(X + o);
-    }, SyncBlock{});
-  };
-  // visit the outputs of the last stage: g(idx, c, j, masked)
-  auto each = [&](auto&& g) {
-#pragma unroll
-    for (int q = 0; q < P / RL; q++)
-#pragma unroll
-      for (int r = 0; r < RL; r++) {
-        int t, i;
-        F::template out_pos<F::S - 1>(tid, q, r, t, i);
-        const int c = min(c0 + t, Nh - 1);
-        g(q * RL + r, c, i, c >= __ldg(a.tb.cut + i));
-      }
-  };
-  const Cx<T> zero = cx<T>(0, 0);
-  const T mu = a.mu, eta = a.eta;
-  switch (f) {
-    case 0:  // d_rho = -(i kx rho_ux_k + i ky rho_uy_k)                     (:402)
-      each([&](int q, int c, int j, bool m) {
-        const size_t o = (size_t)j * ld + c;
-        const Cx<T> p = m ? zero : ikmul(__ldg(kx + c), ldg(a.in[1] + o));
-        const Cx<T> s = m ? zero : ikmul(__ldg(ky + j), ldg(a.in[2] + o));
-        d[q] = -(p + s);
-      });
-      break;
-    case 1:  // -(i kx Mxx + i ky Mxy) - mu (kx^2 + ky^2) ux_k + Fx_k       (:405-406)
-    case 2:  // -(i kx Mxy + i ky Myy) - mu (kx^2 + ky^2) uy_k + Fy_k       (:408-409)
-      fft(a.X[f == 1 ? XMXX : XMXY]);
-      each([&](int q, int c, int j, bool m) { d[q] = m ? zero : ikmul(__ldg(kx + c), v[q]); });
-      fft(a.X[f == 1 ? XMXY : XMYY]);
-      each([&](int q, int c, int j, bool m) { d[q] = -(d[q] + (m ? zero : ikmul(__ldg(ky + j), v[q]))); });
-      fft(a.X[f == 1 ? XUX : XUY]);
-      each([&](int q, int c, int j, bool m) {
-        const T k1 = __ldg(kx + c), k2 = __ldg(ky + j);
-        const Cx<T> p = m ? zero : rmul(k1 * k1, v[q]);
-        const Cx<T> s = m ? zero : rmul(k2 * k2, v[q]);
-        d[q] = d[q] - rmul(mu, p + s);
-      });
-      if (a.forcing) {
-        fft(a.X[f == 1 ? XFX : XFY]);
-        each([&](int q, int, int, bool) { d[q] = d[q] + v[q]; });
-      }
-      if (a.closure) {  // -(i kx tau_x. + i ky tau_.y), masked like the fluxes
-        const Cx<T>* ta = a.clos[f == 1 ? 0 : 1];
-        const Cx<T>* tb = a.clos[f == 1 ? 1 : 2];
-        each([&](int q, int c, int j, bool m) {
-          const size_t o = (size_t)j * ld + c;
-          if (!m) d[q] = d[q] - (ikmul(__ldg(kx + c), ldg(ta + o)) + ikmul(__ldg(ky + j), ldg(tb + o)));
-        });
-      }
-      break;
-    case 3:  // -(i kx Ex + i ky Ey) + mu E_Visc_k                          (:412-413)
-      fft(a.X[XEX], a.X[XEX2]);
-      each([&](int q, int c, int j, bool m) { d[q] = m ? zero : ikmul(__ldg(kx + c), v[q]); });
-      fft(a.X[XEY], a.X[XEY2]);
-      each([&](int q, int c, int j, bool m) { d[q] = -(d[q] + (m ? zero : ikmul(__ldg(ky + j), v[q]))); });
-      fft(a.X[XEV]);
-      each([&](int q, int c, int j, bool m) { d[q] = d[q] + rmul(mu, m ? zero : v[q]); });
-      break;
-    default:  // 4: -i ky Mag_x - eta k^2 Bx ; 5: -i kx Mag_y - eta k^2 By    (:416-417)
-      fft(a.X[XMAG]);
-      each([&](int q, int c, int j, bool m) {
-        const size_t o = (size_t)j * ld + c;
-        const T k1 = __ldg(kx + c), k2 = __ldg(ky + j);
-        const Cx<T> B = ldg(a.in[f] + o);
-        // Mag_y_k = -Mag_x_k exactly
-        const Cx<T> nl = m ? zero : (f == 4 ? ikmul(k2, v[q]) : ikmul(k1, -v[q]));
-        const Cx<T> p = m ? zero : rmul(k1 * k1, B);
-        const Cx<T> s = m ? zero : rmul(k2 * k2, B);
-        d[q] = -nl - rmul(eta, p + s);
-        if (a.closure && !m) {  // subgrid EMF: -i ky EMF (Bx), +i kx EMF (By)
-          const Cx<T> e = ldg(a.clos[3] + o);
-          d[q] = f == 4 ? d[q] - ikmul(k2, e) : d[q] + ikmul(k1, e);
-        }
-      });
-      break;
-  }
-  step_apply_n<T, P>(a.step, f, [&](int e, size_t& idx) {
-    int t, i;
-    F::template out_pos<F::S - 1>(tid, e / RL, e % RL, t, i);
-    const int c = c0 + t;
-    idx = (size_t)i * ld + c;
-    return c < Nh;
-  }, d, a.fuse ? d : nullptr);
-  if (!a.fuse) return;
-  // y-inverse of the next RHS input of these columns (it is in d, at the
-  // forward transform's output positions): through the exchange tile, then
-  // an inverse transform, stored as the next column-inverse pass would
-  auto invert = [&](Cx<T>* dst, int mul) {
-    __syncthreads();  // the exchange tile is free
-#pragma unroll
-    for (int e = 0; e < P; e++) {
-      int t, i;
-      F::template out_pos<F::S - 1>(tid, e / RL, e % RL, t, i);
-      sm[F::sidx(t, i)] = d[e];
-    }
-    __syncthreads();
-    fft_run<F, +1>(sm, tid, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) {
-      return apply_ymul(mul, __ldg(ky + i), sm[F::sidx(t, i)]);
-    }, SyncBlock{});
-    fft_emit<F>(tid, v, [&](int t, int i, Cx<T> x) {
-      const int c = c0 + t;
-      if (c < Nh) st(dst + (size_t)i * ld + c, x);
-    });
-  };
-  invert(a.hnext[f], MUL_ONE);
-  if (f == 4 && a.hikybx) invert(a.hikybx, MUL_IKY);
+#include "col_fwd_com_body.inc"
+}
+
+// The same pass as a device function: output field f, kx columns c0 .., by
+// the CB*L/P threads of the calling CTA (persistent ensemble kernels).
+template <class T, int L, int CB, int P>
+__device__ __forceinline__ void col_fwd_com_tile(const ColFwdComArgs<T>& a, int f, int c0) {
+  using F = FFTB<L, CB, P>;
+  constexpr int RL = F::Pl::R[F::S - 1];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+#include "col_fwd_com_body.inc"
 }
 
 template <int L, class T>

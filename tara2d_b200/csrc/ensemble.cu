@@ -1,34 +1,55 @@
-// Batched ensembles: many independent hydro (*2coh) runs of different grid
-// sizes and viscosities advanced together.
+// Batched ensembles: many independent hydro (*2coh) and MHD (*2com) runs of
+// different grid sizes and viscosities advanced together.
 //
 // Layout: one arena holds every member's fields back to back, each member a
-// block of 20 fields [u_A(3) u_B(3) dold(3) | H(8) X(3)] in its own [N][ld]
-// layout; a device table of member descriptors (the argument blocks of the
-// three RHS phases, with the state buffers of both parities) drives three
-// persistent kernels per step:
+// block in its own [N][ld] layout: hydro 20 fields [u_A(3) u_B(3) dold(3) |
+// H(8) X(3)], MHD 38 fields [u_A(6) u_B(6) dold(6) | H(7) X(13)].  Device
+// tables of member descriptors (the argument blocks of every RHS phase, with
+// the state buffers of both parities) drive persistent kernels per step.
+// Hydro members, three launches:
 //
 //   k_ens_col_inv  items (member, column tile, job): y-inverse, 8 jobs/member
 //   k_ens_row      items (member, block of rows): the hydro row pass
 //   k_ens_col_fwd  items (member, column tile, field): y-forward, mask, AB2
 //
+// MHD members, four launches (a fifth, the column inverse, only where the
+// half-real fields do not hold the y-inverse of the state yet: the column
+// forward pass writes it for the next step, as in a single-grid session):
+//
+//   k_ens_com_inv   items (member, column tile, job): y-inverse of 6 fields
+//   k_ens_com_row1  items (member, block of rows): c2r, fluxes, 8 r2c
+//   k_ens_com_rt    items (member, column tile): d(uy)/dy round trip
+//   k_ens_com_row2  items (member, block of rows): curl-B and (div u)^2 terms
+//   k_ens_com_fwd   items (member, column tile, field): y-forward, assembly,
+//                   AB2/Euler update, y-inverse of the new state
+//
 // Each kernel runs a grid of (CTAs per SM) x (SMs) CTAs that walk a
 // size-sorted item list (largest grids first), so members of every size share
 // every launch; the phase boundaries are the only synchronisation.  A step is
-// the same three launches for any mix of members, so step pairs are captured
-// once into a CUDA graph and replayed.  Per-member arithmetic is the same
+// the same launches for any mix of members (three for the hydro members, four
+// for the MHD ones), so step pairs are captured once into a CUDA graph and
+// replayed.  Per-member arithmetic is the same
 // device code as a single-grid session (col_inv_tile, row_coh_rows,
 // col_fwd_simple_tile), so with the session's values-per-thread choice a
 // member's state is bit-identical to a session run of that member.
 //
-// Tuning (the autotuner picks by timing): values per thread of the column
-// passes and of the row pass (8 or 16; 384-point transforms always use 24)
-// and CTAs per SM of each persistent grid.
+// Tuning (the autotuner picks by timing, hydro phases): values per thread of
+// the column passes and of the row pass (8 or 16; 384-point transforms always
+// use 24) and CTAs per SM of each persistent grid.  The MHD phases use the
+// single-grid sessions' values per thread (ColCfg, ColFwdComCfg, RowCfg) in
+// CTAs of 128 threads, so an MHD member is bit-identical to a session run.
+//
+// The MHD per-member arithmetic is the single-grid device code
+// (col_inv_tile, row_com1_rows, col_rt_tile, row_com2_rows,
+// col_fwd_com_tile), reading its argument block from the member table in
+// global memory; no pointer or tensor map is staged through shared memory.
 #include <algorithm>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <vector>
 #include "coh_impl.cuh"
+#include "com_impl.cuh"
 #include "diag.cuh"
 
 using namespace tara;
@@ -134,6 +155,167 @@ __global__ void __launch_bounds__(kEnsColThreads, 2) k_ens_col_fwd(const EnsMemb
   }
 }
 
+// ---------------------------------------------------------------- MHD members
+constexpr int kEnsComThreads = 128;
+constexpr int kEnsComFields = 38;
+enum { EC_UA = 0, EC_UB = 6, EC_DOLD = 12, EC_H = 18, EC_X = 25 };
+
+// Tile geometry per grid size, with the sessions' values per thread: every
+// item is one CTA of kEnsComThreads threads.
+template <class T, int L> struct EnsComInv {  // column inverse and d(uy)/dy round trip
+  static constexpr int P = ColCfg<T, L>::P;
+  static constexpr int CB = kEnsComThreads * P / L;
+  static_assert(CB * L / P == kEnsComThreads, "column tile does not fill the CTA");
+};
+template <class T, int L> struct EnsComFwd {  // column forward pass
+  static constexpr int P = ColFwdComCfg<T, L>::P;
+  static constexpr int CB = kEnsComThreads * P / L;
+  static_assert(CB * L / P == kEnsComThreads, "column tile does not fill the CTA");
+};
+template <int N> struct EnsComRow {  // rows per item of the two row passes
+  static constexpr int M = N / 2, P = RowCfg<M>::P;
+  static constexpr int R1 = kEnsComThreads / (8 * (M / P));
+  static constexpr int R2 = kEnsComThreads / (4 * (M / P));
+  static_assert(R1 * 8 * (M / P) == kEnsComThreads && R2 * 4 * (M / P) == kEnsComThreads,
+                "row block does not fill the CTA");
+};
+
+template <class T> struct EnsComMember {
+  ColInvArgs<T> inv[2];      // parity p: jobs read the state in buffer p
+  RowCom1Args<T> row1;
+  ColRtArgs<T> rt;
+  RowCom2Args<T> row2;
+  ColFwdComArgs<T> fwd[2];   // parity p: state p -> state 1-p, history, half-real fields of state 1-p
+  int N;
+};
+
+// registers: FP32 members fit 128 per thread (4 CTAs per SM), FP64 ones get up to 255
+template <class T> constexpr int ens_com_minb() { return sizeof(T) == 4 ? 4 : 2; }
+
+#define TARA_ENS_COM_SIZES(FN) \
+  case 128: FN(128); break;    \
+  case 256: FN(256); break;    \
+  case 384: FN(384); break;    \
+  case 512: FN(512); break;
+
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_inv(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems, int parity) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    const EnsComMember<T>& m = mem[w.x];
+    const ColInvArgs<T>& a = m.inv[parity];
+#define TARA_EC_INV(L)                                                                                   \
+  col_inv_tile<T, L, EnsComInv<T, L>::CB, EnsComInv<T, L>::P>(a.job[w.z], a.tb, w.y * EnsComInv<T, L>::CB, sm, \
+                                                              threadIdx.x)
+    switch (m.N) { TARA_ENS_COM_SIZES(TARA_EC_INV) }
+#undef TARA_EC_INV
+    __syncthreads();
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_row1(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    const EnsComMember<T>& m = mem[w.x];
+#define TARA_EC_ROW1(N) \
+  row_com1_rows<T, EnsComRow<N>::M, EnsComRow<N>::P, false>(m.row1, w.y * EnsComRow<N>::R1)
+    switch (m.N) { TARA_ENS_COM_SIZES(TARA_EC_ROW1) }
+#undef TARA_EC_ROW1
+    __syncthreads();
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_rt(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    const EnsComMember<T>& m = mem[w.x];
+#define TARA_EC_RT(L) col_rt_tile<T, L, EnsComInv<T, L>::CB, EnsComInv<T, L>::P>(m.rt, w.y * EnsComInv<T, L>::CB)
+    switch (m.N) { TARA_ENS_COM_SIZES(TARA_EC_RT) }
+#undef TARA_EC_RT
+    __syncthreads();
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_row2(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    const EnsComMember<T>& m = mem[w.x];
+#define TARA_EC_ROW2(N) row_com2_rows<T, EnsComRow<N>::M, EnsComRow<N>::P, 0>(m.row2, w.y * EnsComRow<N>::R2)
+    switch (m.N) { TARA_ENS_COM_SIZES(TARA_EC_ROW2) }
+#undef TARA_EC_ROW2
+    __syncthreads();
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_fwd(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems, int parity) {
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = items[it];
+    const EnsComMember<T>& m = mem[w.x];
+#define TARA_EC_FWD(L) \
+  col_fwd_com_tile<T, L, EnsComFwd<T, L>::CB, EnsComFwd<T, L>::P>(m.fwd[parity], w.z, w.y * EnsComFwd<T, L>::CB)
+    switch (m.N) { TARA_ENS_COM_SIZES(TARA_EC_FWD) }
+#undef TARA_EC_FWD
+    __syncthreads();
+  }
+}
+
+// dynamic shared memory of each MHD phase kernel: the largest over the sizes
+template <class T> size_t ens_com_col_smem() {
+  size_t m = 0;
+#define TARA_EC_CS(L)                                                                                    \
+  m = std::max(m, (size_t)FFTB<L, EnsComInv<T, L>::CB, EnsComInv<T, L>::P>::SMEM_ELEMS);              \
+  m = std::max(m, (size_t)FFTB<L, EnsComFwd<T, L>::CB, EnsComFwd<T, L>::P>::SMEM_ELEMS)
+  TARA_EC_CS(128);
+  TARA_EC_CS(256);
+  TARA_EC_CS(384);
+  TARA_EC_CS(512);
+#undef TARA_EC_CS
+  return m * sizeof(Cx<T>);
+}
+template <class T> size_t ens_com_row_smem(int pass) {
+  size_t m = 0;
+#define TARA_EC_RS(N)                                                                               \
+  m = std::max(m, (size_t)(pass == 1 ? EnsComRow<N>::R1 * 8 : EnsComRow<N>::R2 * 5) *                 \
+                      RowFFT<EnsComRow<N>::M, EnsComRow<N>::P>::SMEM_ELEMS)
+  TARA_EC_RS(128);
+  TARA_EC_RS(256);
+  TARA_EC_RS(384);
+  TARA_EC_RS(512);
+#undef TARA_EC_RS
+  return m * sizeof(Cx<T>);
+}
+template <class T> int ens_com_inv_cb(int N) {
+  switch (N) {
+    case 128: return EnsComInv<T, 128>::CB;
+    case 256: return EnsComInv<T, 256>::CB;
+    case 384: return EnsComInv<T, 384>::CB;
+    default: return EnsComInv<T, 512>::CB;
+  }
+}
+template <class T> int ens_com_fwd_cb(int N) {
+  switch (N) {
+    case 128: return EnsComFwd<T, 128>::CB;
+    case 256: return EnsComFwd<T, 256>::CB;
+    case 384: return EnsComFwd<T, 384>::CB;
+    default: return EnsComFwd<T, 512>::CB;
+  }
+}
+inline int ens_com_rows(int N, int pass) {
+  switch (N) {
+    case 128: return pass == 1 ? EnsComRow<128>::R1 : EnsComRow<128>::R2;
+    case 256: return pass == 1 ? EnsComRow<256>::R1 : EnsComRow<256>::R2;
+    case 384: return pass == 1 ? EnsComRow<384>::R1 : EnsComRow<384>::R2;
+    default: return pass == 1 ? EnsComRow<512>::R1 : EnsComRow<512>::R2;
+  }
+}
+
 template <class T, int PC> size_t ens_col_smem() {
   size_t m = 0;
   m = std::max(m, (size_t)FFTB<128, EnsCol<128, PC>::CB, EnsCol<128, PC>::P>::SMEM_ELEMS);
@@ -182,7 +364,7 @@ struct tara_ensemble {
       if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
   }
-  virtual int init(const int* N, const tara_params* p) = 0;
+  virtual int init(const int* models, const int* N, const tara_params* p) = 0;
   virtual int set_state(int m, const double* const* f, int which) = 0;
   virtual int get_state(int m, double* const* f, int which) = 0;
   virtual int step(int stepper, int nsteps) = 0;
@@ -192,6 +374,7 @@ struct tara_ensemble {
   virtual int save_state(bool restore) = 0;
   virtual int diagnostics(int m, double* out, int nout, double* Ek, int nbins) = 0;
   virtual int num_shells(int m) = 0;
+  virtual int num_fields(int m) const = 0;
   virtual int device_status() = 0;
 };
 
@@ -200,6 +383,9 @@ namespace {
 template <class T>
 struct EnsembleT : tara_ensemble {
   std::vector<int> N;
+  std::vector<int> model;                                 // TARA_MODEL_COH or TARA_MODEL_COM per member
+  std::vector<int> slot;                                  // index of the member in hmem or hcom
+  int nhyd = 0, ncom = 0;
   std::vector<tara_params> prm;
   std::map<int, std::unique_ptr<Grid<T>>> grids;        // tables per grid size
   std::map<int, std::unique_ptr<DiagWork<T>>> diags;
@@ -208,10 +394,17 @@ struct EnsembleT : tara_ensemble {
   Cx<T>* arena = nullptr;
   double* stage = nullptr;                                // FP64 host-layout staging (largest member)
   double* drec = nullptr;                                 // one diagnostics record
-  EnsMember<T>* dmem = nullptr;
+  EnsMember<T>* dmem = nullptr;                           // hydro member table
   std::vector<EnsMember<T>> hmem;
   int4* ditems[3] = {nullptr, nullptr, nullptr};
   int nitems[3] = {0, 0, 0};
+  EnsComMember<T>* dcom = nullptr;                        // MHD member table
+  std::vector<EnsComMember<T>> hcom;
+  int4* citems[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // inv, row1, rt, row2, fwd
+  int ncitems[5] = {0, 0, 0, 0, 0};
+  // the MHD members' half-real fields hold the y-inverse of their current
+  // state (written by the previous column forward pass)
+  bool com_h_valid = false;
   int tuning[6] = {16, 16, 16, 0, 0, 0};  // P col_inv, P row, P col_fwd, CTAs/SM of each (0 = most that fit)
   int parity = 0;
   int built_mode = -1;
@@ -228,7 +421,10 @@ struct EnsembleT : tara_ensemble {
     for (auto& g : grids) g.second->release();
     for (auto& p : ditems)
       if (p) cudaFree(p);
+    for (auto& p : citems)
+      if (p) cudaFree(p);
     if (dmem) cudaFree(dmem);
+    if (dcom) cudaFree(dcom);
     if (arena) cudaFree(arena);
     if (stage) cudaFree(stage);
     if (drec) cudaFree(drec);
@@ -241,17 +437,30 @@ struct EnsembleT : tara_ensemble {
   }
   Cx<T>* field(int m, int f) const { return arena + off[m] + (size_t)f * elems[m]; }
 
-  int init(const int* Nin, const tara_params* p) override {
+  int nfields(int m) const { return model[m] == TARA_MODEL_COM ? 6 : 3; }
+  int num_fields(int m) const override { return m >= 0 && m < n ? nfields(m) : 0; }
+  int init(const int* models, const int* Nin, const tara_params* p) override {
     N.assign(Nin, Nin + n);
+    model.assign(models, models + n);
     prm.assign(p, p + n);
     size_t total = 0, maxh = 0;
     off.resize(n);
     elems.resize(n);
+    slot.resize(n);
     for (int m = 0; m < n; m++) {
       if (N[m] != 128 && N[m] != 256 && N[m] != 384 && N[m] != 512) {
         set_error("ensemble member grid sizes must be 128, 256, 384 or 512");
         return TARA_EUNSUPPORTED;
       }
+      if (model[m] != TARA_MODEL_COH && model[m] != TARA_MODEL_COM) {
+        set_error("ensemble members run the hydro or the MHD model");
+        return TARA_EUNSUPPORTED;
+      }
+      if (model[m] == TARA_MODEL_COM && (p[m].A != 0.0 || p[m].fix_curlB != 0)) {
+        set_error("MHD ensemble members run without forcing (A = 0) and with curl B as the reference builds it");
+        return TARA_EUNSUPPORTED;
+      }
+      slot[m] = model[m] == TARA_MODEL_COM ? ncom++ : nhyd++;
       auto& g = grids[N[m]];
       if (!g) {
         g.reset(new Grid<T>());
@@ -262,7 +471,7 @@ struct EnsembleT : tara_ensemble {
       }
       off[m] = total;
       elems[m] = g->field_elems();
-      total += elems[m] * kEnsFields;
+      total += elems[m] * (model[m] == TARA_MODEL_COM ? kEnsComFields : kEnsFields);
       maxh = std::max(maxh, (size_t)(N[m] / 2 + 1) * N[m]);
     }
     if (cudaMalloc(&arena, total * sizeof(Cx<T>)) != cudaSuccess) {
@@ -273,18 +482,90 @@ struct EnsembleT : tara_ensemble {
     TARA_CUDA_TRY(cudaMemsetAsync(arena, 0, total * sizeof(Cx<T>), st));
     TARA_CUDA_TRY(cudaMalloc(&stage, maxh * sizeof(Cx<double>)));
     TARA_CUDA_TRY(cudaMalloc(&drec, (kDiagOut + 1024) * sizeof(double)));
-    TARA_CUDA_TRY(cudaMalloc(&dmem, (size_t)n * sizeof(EnsMember<T>)));
+    if (nhyd) TARA_CUDA_TRY(cudaMalloc(&dmem, (size_t)nhyd * sizeof(EnsMember<T>)));
+    if (ncom) TARA_CUDA_TRY(cudaMalloc(&dcom, (size_t)ncom * sizeof(EnsComMember<T>)));
     build_members();
-    TARA_CUDA_TRY(cudaMemcpyAsync(dmem, hmem.data(), (size_t)n * sizeof(EnsMember<T>), cudaMemcpyHostToDevice, st));
+    TARA_TRY(upload_members());
     TARA_TRY(build_items());
     TARA_CUDA_TRY(cudaStreamSynchronize(st));
     return TARA_OK;
   }
 
+  int upload_members() {
+    if (nhyd)
+      TARA_CUDA_TRY(cudaMemcpyAsync(dmem, hmem.data(), (size_t)nhyd * sizeof(EnsMember<T>), cudaMemcpyHostToDevice, st));
+    if (ncom)
+      TARA_CUDA_TRY(cudaMemcpyAsync(dcom, hcom.data(), (size_t)ncom * sizeof(EnsComMember<T>), cudaMemcpyHostToDevice,
+                                    st));
+    return TARA_OK;
+  }
+  // argument blocks of an MHD member (src/derive2com.f95 per member)
+  void build_com_member(int m) {
+    EnsComMember<T>& e = hcom[slot[m]];
+    const Tables<T>& tb = grids[N[m]]->tb;
+    const tara_params& q = prm[m];
+    e.N = N[m];
+    Cx<T>* H[7];
+    Cx<T>* X[13];
+    for (int k = 0; k < 7; k++) H[k] = field(m, EC_H + k);
+    for (int k = 0; k < 13; k++) X[k] = field(m, EC_X + k);
+    for (int par = 0; par < 2; par++) {
+      const int ubase = par ? EC_UB : EC_UA, nbase = par ? EC_UA : EC_UB;
+      e.inv[par].tb = tb;
+      for (int k = 0; k < 6; k++) e.inv[par].job[k] = ColInvJob<T>{field(m, ubase + k), H[k], MUL_ONE, (T)0};
+      ColFwdComArgs<T>& f = e.fwd[par];
+      f.tb = tb;
+      for (int k = 0; k < 13; k++) f.X[k] = X[k];
+      for (int k = 0; k < 6; k++) {
+        f.in[k] = field(m, ubase + k);
+        f.hnext[k] = H[k];
+        f.step.u[k] = field(m, ubase + k);
+        f.step.unew[k] = field(m, nbase + k);
+        f.step.dold[k] = field(m, EC_DOLD + k);
+      }
+      f.mu = (T)q.mu;
+      f.eta = (T)q.eta;
+      f.forcing = 0;
+      f.closure = 0;
+      f.fuse = 1;
+      f.hikybx = nullptr;
+      f.step.dt = (T)q.dt;
+      f.step.scale = nullptr;
+    }
+    RowCom1Args<T>& r1 = e.row1;
+    r1.tb = tb;
+    for (int k = 0; k < 6; k++) r1.H[k] = H[k];
+    for (int k = 0; k < 11; k++) r1.X[k] = X[k];
+    r1.cs2 = (T)(q.CS * q.CS);
+    r1.rb = ens_com_rows(N[m], 1);
+    r1.cfl = CflRow{nullptr, 0.0, 0.0, 0.0};
+    e.rt.tb = tb;
+    e.rt.src = X[XUY];
+    e.rt.dst = H[HDUY];
+    e.rt.mul = MUL_IKY;
+    RowCom2Args<T>& r2 = e.row2;
+    r2.tb = tb;
+    r2.Xux = X[XUX];
+    r2.Hduy = H[HDUY];
+    r2.Hbx = H[HBX];
+    r2.Hby = H[HBY];
+    r2.Hikybx = nullptr;
+    r2.Xex2 = X[XEX2];
+    r2.Xey2 = X[XEY2];
+    r2.Xev = X[XEV];
+    r2.eta = (T)q.eta;
+    r2.inv_nx = (T)(1.0 / N[m]);
+    r2.rb = ens_com_rows(N[m], 2);
+  }
   void build_members() {
-    hmem.assign(n, EnsMember<T>{});
+    hmem.assign(nhyd, EnsMember<T>{});
+    hcom.assign(ncom, EnsComMember<T>{});
     for (int m = 0; m < n; m++) {
-      EnsMember<T>& e = hmem[m];
+      if (model[m] == TARA_MODEL_COM) {
+        build_com_member(m);
+        continue;
+      }
+      EnsMember<T>& e = hmem[slot[m]];
       const Tables<T>& tb = grids[N[m]]->tb;
       e.N = N[m];
       const int src[8] = {0, 0, 1, 1, 1, 2, 2, 2};
@@ -316,7 +597,9 @@ struct EnsembleT : tara_ensemble {
     if (mode == built_mode) return TARA_OK;
     for (auto& e : hmem)
       for (auto& f : e.fwd) f.step.mode = mode;
-    TARA_CUDA_TRY(cudaMemcpyAsync(dmem, hmem.data(), (size_t)n * sizeof(EnsMember<T>), cudaMemcpyHostToDevice, st));
+    for (auto& e : hcom)
+      for (auto& f : e.fwd) f.step.mode = mode;
+    TARA_TRY(upload_members());
     built_mode = mode;
     return TARA_OK;
   }
@@ -325,25 +608,43 @@ struct EnsembleT : tara_ensemble {
     std::vector<int> order(n);
     for (int m = 0; m < n; m++) order[m] = m;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return N[a] > N[b]; });
-    std::vector<int4> it[3];
+    std::vector<int4> it[3], ic[5];
     for (int m : order) {
       const int Nh = N[m] / 2 + 1;
+      if (model[m] == TARA_MODEL_COM) {
+        const int s = slot[m];
+        const int ti = (Nh + ens_com_inv_cb<T>(N[m]) - 1) / ens_com_inv_cb<T>(N[m]);
+        const int tf = (Nh + ens_com_fwd_cb<T>(N[m]) - 1) / ens_com_fwd_cb<T>(N[m]);
+        for (int t = 0; t < ti; t++)
+          for (int j = 0; j < 6; j++) ic[0].push_back(make_int4(s, t, j, 0));
+        for (int r = 0; r < N[m] / ens_com_rows(N[m], 1); r++) ic[1].push_back(make_int4(s, r, 0, 0));
+        for (int t = 0; t < ti; t++) ic[2].push_back(make_int4(s, t, 0, 0));
+        for (int r = 0; r < N[m] / ens_com_rows(N[m], 2); r++) ic[3].push_back(make_int4(s, r, 0, 0));
+        for (int t = 0; t < tf; t++)
+          for (int f = 0; f < 6; f++) ic[4].push_back(make_int4(s, t, f, 0));
+        continue;
+      }
+      const int hs = slot[m];
       const int ti = (Nh + ens_cb(N[m], tuning[0]) - 1) / ens_cb(N[m], tuning[0]);
       for (int t = 0; t < ti; t++)
-        for (int j = 0; j < 8; j++) it[0].push_back(make_int4(m, t, j, 0));
+        for (int j = 0; j < 8; j++) it[0].push_back(make_int4(hs, t, j, 0));
       const int rows = ens_rows(N[m], tuning[1]);
-      for (int r = 0; r < N[m] / rows; r++) it[1].push_back(make_int4(m, r, 0, 0));
+      for (int r = 0; r < N[m] / rows; r++) it[1].push_back(make_int4(hs, r, 0, 0));
       const int tf = (Nh + ens_cb(N[m], tuning[2]) - 1) / ens_cb(N[m], tuning[2]);
       for (int t = 0; t < tf; t++)
-        for (int f = 0; f < 3; f++) it[2].push_back(make_int4(m, t, f, 0));
+        for (int f = 0; f < 3; f++) it[2].push_back(make_int4(hs, t, f, 0));
     }
-    for (int k = 0; k < 3; k++) {
-      if (ditems[k]) cudaFree(ditems[k]);
-      ditems[k] = nullptr;
-      nitems[k] = (int)it[k].size();
-      TARA_CUDA_TRY(cudaMalloc(&ditems[k], it[k].size() * sizeof(int4)));
-      TARA_CUDA_TRY(cudaMemcpyAsync(ditems[k], it[k].data(), it[k].size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-    }
+    auto upload = [&](std::vector<int4>& v, int4*& d, int& nd) -> int {
+      if (d) cudaFree(d);
+      d = nullptr;
+      nd = (int)v.size();
+      if (v.empty()) return TARA_OK;
+      TARA_CUDA_TRY(cudaMalloc(&d, v.size() * sizeof(int4)));
+      TARA_CUDA_TRY(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+      return TARA_OK;
+    };
+    for (int k = 0; k < 3; k++) TARA_TRY(upload(it[k], ditems[k], nitems[k]));
+    for (int k = 0; k < 5; k++) TARA_TRY(upload(ic[k], citems[k], ncitems[k]));
     TARA_CUDA_TRY(cudaStreamSynchronize(st));
     return TARA_OK;
   }
@@ -359,6 +660,7 @@ struct EnsembleT : tara_ensemble {
     return TARA_OK;
   }
   int launch_inv(int par) {
+    if (!nitems[0]) return TARA_OK;
     int grid = 0;
     if (tuning[0] == 8) {
       const size_t smem = ens_col_smem<T, 8>();
@@ -372,6 +674,7 @@ struct EnsembleT : tara_ensemble {
     return TARA_OK;
   }
   int launch_row() {
+    if (!nitems[1]) return TARA_OK;
     int grid = 0;
     if (tuning[1] == 8) {
       const size_t smem = ens_row_smem<T, 8>();
@@ -385,6 +688,7 @@ struct EnsembleT : tara_ensemble {
     return TARA_OK;
   }
   int launch_fwd(int par) {
+    if (!nitems[2]) return TARA_OK;
     int grid = 0;
     if (tuning[2] == 8) {
       const size_t smem = ens_col_smem<T, 8>();
@@ -397,11 +701,55 @@ struct EnsembleT : tara_ensemble {
     }
     return TARA_OK;
   }
+  // MHD phase ph (0 column inverse, 1 row pass 1, 2 d(uy)/dy, 3 row pass 2,
+  // 4 column forward + update) over every MHD member
+  int launch_com(int ph, int par) {
+    if (!ncitems[ph]) return TARA_OK;
+    int grid = 0;
+    const int ni = ncitems[ph];
+    switch (ph) {
+      case 0: {
+        const size_t smem = ens_com_col_smem<T>();
+        TARA_TRY(grid_of(k_ens_com_inv<T>, kEnsComThreads, smem, 0, grid));
+        k_ens_com_inv<T><<<std::min(grid, ni), kEnsComThreads, smem, st>>>(dcom, citems[0], ni, par);
+        break;
+      }
+      case 1: {
+        const size_t smem = ens_com_row_smem<T>(1);
+        TARA_TRY(grid_of(k_ens_com_row1<T>, kEnsComThreads, smem, 0, grid));
+        k_ens_com_row1<T><<<std::min(grid, ni), kEnsComThreads, smem, st>>>(dcom, citems[1], ni);
+        break;
+      }
+      case 2: {
+        const size_t smem = ens_com_col_smem<T>();
+        TARA_TRY(grid_of(k_ens_com_rt<T>, kEnsComThreads, smem, 0, grid));
+        k_ens_com_rt<T><<<std::min(grid, ni), kEnsComThreads, smem, st>>>(dcom, citems[2], ni);
+        break;
+      }
+      case 3: {
+        const size_t smem = ens_com_row_smem<T>(2);
+        TARA_TRY(grid_of(k_ens_com_row2<T>, kEnsComThreads, smem, 0, grid));
+        k_ens_com_row2<T><<<std::min(grid, ni), kEnsComThreads, smem, st>>>(dcom, citems[3], ni);
+        break;
+      }
+      default: {
+        const size_t smem = ens_com_col_smem<T>();
+        TARA_TRY(grid_of(k_ens_com_fwd<T>, kEnsComThreads, smem, 0, grid));
+        k_ens_com_fwd<T><<<std::min(grid, ni), kEnsComThreads, smem, st>>>(dcom, citems[4], ni, par);
+        break;
+      }
+    }
+    return TARA_OK;
+  }
   int launch_steps(int n_) {
     for (int s = 0; s < n_; s++) {
       TARA_TRY(launch_inv(parity));
       TARA_TRY(launch_row());
       TARA_TRY(launch_fwd(parity));
+      if (ncom) {
+        for (int ph = com_h_valid ? 1 : 0; ph < 5; ph++) TARA_TRY(launch_com(ph, parity));
+        com_h_valid = true;  // the column forward pass wrote the y-inverse of the new state
+      }
       TARA_CUDA_TRY(cudaGetLastError());
       parity ^= 1;
     }
@@ -418,7 +766,13 @@ struct EnsembleT : tara_ensemble {
       TARA_TRY(set_mode(mode));
     }
     int done = 0;
-    if (nsteps >= 2) {
+    if (ncom && !com_h_valid && nsteps > 0) {
+      // the MHD members' first step includes their column inverse; captured
+      // step pairs start from half-real fields written by a step
+      TARA_TRY(launch_steps(1));
+      done = 1;
+    }
+    if (nsteps - done >= 2) {
       if (!graph || graph_mode != mode || graph_parity != parity) {
         drop_graph();
         const int p0 = parity;
@@ -484,7 +838,7 @@ struct EnsembleT : tara_ensemble {
   // copy of every member's state and AB2 history (restore = true puts it back)
   int save_state(bool restore) override {
     size_t need = 0;
-    for (int m = 0; m < n; m++) need += 9 * elems[m];
+    for (int m = 0; m < n; m++) need += 3 * nfields(m) * elems[m];
     if (!restore) {
       if (!backup) {
         if (cudaMalloc(&backup, need * sizeof(Cx<T>)) != cudaSuccess) {
@@ -500,17 +854,18 @@ struct EnsembleT : tara_ensemble {
       return TARA_EINVAL;
     }
     size_t o = 0;
-    for (int m = 0; m < n; m++) {
-      const size_t b = 9 * elems[m] * sizeof(Cx<T>);
+    for (int m = 0; m < n; m++) {  // u_A, u_B, history: the first 3 nf fields of the member's block
+      const size_t b = 3 * nfields(m) * elems[m] * sizeof(Cx<T>);
       if (restore) TARA_CUDA_TRY(cudaMemcpyAsync(field(m, 0), backup + o, b, cudaMemcpyDeviceToDevice, st));
       else TARA_CUDA_TRY(cudaMemcpyAsync(backup + o, field(m, 0), b, cudaMemcpyDeviceToDevice, st));
-      o += 9 * elems[m];
+      o += 3 * nfields(m) * elems[m];
     }
     TARA_CUDA_TRY(cudaStreamSynchronize(st));
     if (restore) {
       cudaFree(backup);
       backup = nullptr;
       parity = saved_parity;
+      com_h_valid = false;
       drop_graph();
     }
     return TARA_OK;
@@ -534,11 +889,15 @@ struct EnsembleT : tara_ensemble {
   }
 
   // which: 0 state, 1 AB2 history
-  Cx<T>* fptr(int m, int which, int q) { return field(m, which ? EF_DOLD + q : (parity ? EF_UB : EF_UA) + q); }
+  Cx<T>* fptr(int m, int which, int q) {
+    if (model[m] == TARA_MODEL_COM) return field(m, which ? EC_DOLD + q : (parity ? EC_UB : EC_UA) + q);
+    return field(m, which ? EF_DOLD + q : (parity ? EF_UB : EF_UA) + q);
+  }
   int set_state(int m, const double* const* h, int which) override {
     if (m < 0 || m >= n || !h) { set_error("bad member or null field array"); return TARA_EINVAL; }
     const int Nh = N[m] / 2 + 1, ld = grids[N[m]]->ld;
-    for (int q = 0; q < 3; q++) {
+    if (which == 0 && model[m] == TARA_MODEL_COM) com_h_valid = false;
+    for (int q = 0; q < nfields(m); q++) {
       if (!h[q]) { set_error("null host field pointer"); return TARA_EINVAL; }
       if constexpr (sizeof(T) == sizeof(double)) {
         TARA_CUDA_TRY(cudaMemcpy2DAsync(fptr(m, which, q), ld * sizeof(Cx<T>), h[q], Nh * sizeof(Cx<double>),
@@ -556,7 +915,7 @@ struct EnsembleT : tara_ensemble {
   int get_state(int m, double* const* h, int which) override {
     if (m < 0 || m >= n || !h) { set_error("bad member or null field array"); return TARA_EINVAL; }
     const int Nh = N[m] / 2 + 1, ld = grids[N[m]]->ld;
-    for (int q = 0; q < 3; q++) {
+    for (int q = 0; q < nfields(m); q++) {
       if (!h[q]) { set_error("null host field pointer"); return TARA_EINVAL; }
       if constexpr (sizeof(T) == sizeof(double)) {
         TARA_CUDA_TRY(cudaMemcpy2DAsync(h[q], Nh * sizeof(Cx<double>), fptr(m, which, q), ld * sizeof(Cx<T>),
@@ -586,9 +945,19 @@ struct EnsembleT : tara_ensemble {
       dw.reset(new DiagWork<T>());
       TARA_TRY(dw->alloc(g, st));
     }
-    FieldPool<T> H{field(m, EF_H), elems[m], 8}, X{field(m, EF_X), elems[m], 3};
-    Cx<T>* state[3] = {fptr(m, 0, 0), fptr(m, 0, 1), fptr(m, 0, 2)};
-    TARA_TRY(diag_record(TARA_MODEL_COH, g, *dw, state, H, X, X, drec, st));
+    if (model[m] == TARA_MODEL_COM) {
+      // the half-real and x-transformed work fields are the diagnostics' scratch
+      FieldPool<T> H{field(m, EC_H), elems[m], 7}, X{field(m, EC_X), elems[m], 13};
+      FieldPool<T> spec{field(m, EC_X + 2), elems[m], 2};
+      Cx<T>* state[6];
+      for (int q = 0; q < 6; q++) state[q] = fptr(m, 0, q);
+      com_h_valid = false;
+      TARA_TRY(diag_record(TARA_MODEL_COM, g, *dw, state, H, X, spec, drec, st));
+    } else {
+      FieldPool<T> H{field(m, EF_H), elems[m], 8}, X{field(m, EF_X), elems[m], 3};
+      Cx<T>* state[3] = {fptr(m, 0, 0), fptr(m, 0, 1), fptr(m, 0, 2)};
+      TARA_TRY(diag_record(TARA_MODEL_COH, g, *dw, state, H, X, X, drec, st));
+    }
     std::vector<double> rec(kDiagOut + ns);
     TARA_CUDA_TRY(cudaMemcpyAsync(rec.data(), drec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     TARA_CUDA_TRY(cudaStreamSynchronize(st));
@@ -602,10 +971,10 @@ struct EnsembleT : tara_ensemble {
 
 extern "C" {
 
-int tara_ens_open(tara_ensemble** out, int model, int n, const int* N, const tara_params* params, int precision) {
-  if (!out || !N || !params || n < 1) { set_error("null argument or empty ensemble"); return TARA_EINVAL; }
+int tara_ens_open_mixed(tara_ensemble** out, int n, const int* models, const int* N, const tara_params* params,
+                        int precision) {
+  if (!out || !models || !N || !params || n < 1) { set_error("null argument or empty ensemble"); return TARA_EINVAL; }
   *out = nullptr;
-  if (model != TARA_MODEL_COH) { set_error("ensembles run the hydro model"); return TARA_EUNSUPPORTED; }
   if (precision != TARA_FP32 && precision != TARA_FP64) { set_error("unknown precision"); return TARA_EINVAL; }
   std::unique_ptr<tara_ensemble> e(precision == TARA_FP32 ? (tara_ensemble*)new EnsembleT<float>()
                                                           : (tara_ensemble*)new EnsembleT<double>());
@@ -615,11 +984,22 @@ int tara_ens_open(tara_ensemble** out, int model, int n, const int* N, const tar
     set_error("cudaStreamCreate failed");
     return TARA_ECUDA;
   }
-  const int r = e->init(N, params);
+  const int r = e->init(models, N, params);
   if (r != TARA_OK) return r;
   *out = e.release();
   return TARA_OK;
 }
+int tara_ens_open(tara_ensemble** out, int model, int n, const int* N, const tara_params* params, int precision) {
+  if (!out || n < 1) { set_error("null argument or empty ensemble"); return TARA_EINVAL; }
+  *out = nullptr;
+  if (model != TARA_MODEL_COH && model != TARA_MODEL_COM) {
+    set_error("ensembles run the hydro or the MHD model");
+    return TARA_EUNSUPPORTED;
+  }
+  std::vector<int> models(n, model);
+  return tara_ens_open_mixed(out, n, models.data(), N, params, precision);
+}
+int tara_ens_num_fields(const tara_ensemble* e, int member) { return e ? e->num_fields(member) : 0; }
 int tara_ens_close(tara_ensemble* e) {
   if (!e) return TARA_EINVAL;
   delete e;

@@ -539,23 +539,15 @@ __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_rt(co
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
   const int c0 = blockIdx.x * CB;
-  const int Nh = a.tb.Nh, ld = a.tb.ld;
-  const T* ky = a.tb.ky;
-  Cx<T> v[P];
-  fft_run<F, -1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) -> Cx<T> {
-    const int c = c0 + t;
-    if (c >= Nh) return cx<T>(0, 0);
-    return ldg(a.src + (size_t)i * ld + c);
-  }, SyncBlock{});
-  __syncthreads();
-  fft_emit<F>(threadIdx.x, v, [&](int t, int j, Cx<T> x) { sm[F::sidx(t, j)] = apply_ymul(a.mul, __ldg(ky + j), x); });
-  __syncthreads();
-  fft_run<F, +1>(sm, threadIdx.x, v, TwGlobal<T>{a.tb.tw_col}, [&](int t, int i) { return sm[F::sidx(t, i)]; },
-                 SyncBlock{});
-  fft_emit<F>(threadIdx.x, v, [&](int t, int i, Cx<T> x) {
-    const int c = c0 + t;
-    if (c < Nh) st(a.dst + (size_t)i * ld + c, x);
-  });
+#include "col_rt_body.inc"
+}
+// The same pass as a device function of the calling CTA (CB*L/P threads).
+template <class T, int L, int CB, int P>
+__device__ __forceinline__ void col_rt_tile(const ColRtArgs<T>& a, int c0) {
+  using F = FFTB<L, CB, P>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
+#include "col_rt_body.inc"
 }
 template <int L, class T>
 inline void col_rt_dispatch(const ColRtArgs<T>& a, cudaStream_t st) {

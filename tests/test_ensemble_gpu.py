@@ -94,7 +94,7 @@ def test_ensemble_errors(tara):
     with pytest.raises(tara.TaraError):
         tara.Ensemble([100], p)
     with pytest.raises(tara.TaraError):
-        tara.Ensemble([128], p, model=tara.MODEL_COM)
+        tara.Ensemble([128], p, model=tara.MODEL_CSH)  # ensembles run the hydro and MHD models
     with tara.Ensemble([128], p) as e:
         with pytest.raises(tara.TaraError):
             e.step(tara.STEP_RK4, 1)
