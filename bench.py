@@ -205,20 +205,38 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ ensemble
-def run_ensemble(args):
-    """Side workload (not the headline): 256 seeded hydro runs, N uniform in
+def run_ensemble(args, mixed=False):
+    """Side workload (not the headline): 256 seeded runs, N uniform in
     {128,256,384,512}, nu log-uniform in [1e-4, 1e-2], k0 uniform in [2, 8],
-    FP32 fields, AB2 dt = 1e-4, advanced together; one step = every member
-    one AB2 step.  Compared with the same members run one session at a time."""
+    FP32 fields, advanced together; one step = every member one AB2 step.
+    mixed=False: every member a hydro run (AB2 dt = 1e-4).  mixed=True: even
+    members hydro, odd members MHD (mu = eta = nu, CS = 10, AB2 dt = 2e-5,
+    random-phase u and B).  Compared with the same members run one session
+    at a time."""
     import tara2d_b200 as T
     from tara2d_b200 import initial
     mem = initial.ensemble_members(256, seed=0)
-    params = [T.Params.make(Lx=2 * PI, Ly=2 * PI, pi=PI, mux=d["nu"], muy=d["nu"], ms=1.0, CS=3.77, dt=1e-4)
-              for d in mem]
+    models = [T.MODEL_COM if mixed and m % 2 else T.MODEL_COH for m in range(len(mem))]
+
+    def member_params(m):
+        d = mem[m]
+        if models[m] == T.MODEL_COM:
+            return T.Params.make(Lx=2 * PI, Ly=2 * PI, pi=PI, mu=d["nu"], eta=d["nu"], ms=1.0, CS=10.0,
+                                 spheat=5.0 / 3.0, mu_0=1.0, kf=1.0, A=0.0, dt=2e-5)
+        return T.Params.make(Lx=2 * PI, Ly=2 * PI, pi=PI, mux=d["nu"], muy=d["nu"], ms=1.0, CS=3.77, dt=1e-4)
+
+    def member_state(m):
+        d = mem[m]
+        if models[m] == T.MODEL_COM:
+            return initial.com_random_phase(d["N"], d["N"], seed=d["seed"], k0=d["k0"], CS=10.0)
+        return initial.coh_random_phase(d["N"], d["N"], seed=d["seed"], k0=d["k0"])
+
+    params = [member_params(m) for m in range(len(mem))]
     sizes = [d["N"] for d in mem]
-    ens = T.Ensemble(sizes, params, precision=T.FP32)
-    for m, d in enumerate(mem):
-        ens.set_state(m, initial.coh_random_phase(d["N"], d["N"], seed=d["seed"], k0=d["k0"]))
+    ens = T.Ensemble(sizes, params, precision=T.FP32, model=models)
+    for m in range(len(mem)):
+        ens.set_state(m, member_state(m))
+    ens.step(T.STEP_AB2, 1)
     default_ms = ens.time_steps(T.STEP_AB2, 20) / 20
     tuning, phase_ms = ens.autotune(T.STEP_AB2, reps=3)
     W, K = max(3, args.warmup), max(1, args.steps)
@@ -226,30 +244,38 @@ def run_ensemble(args):
     ms = ens.time_steps(T.STEP_AB2, K)
     # the same members, one session each (graph replay), steps timed per member
     seq_ms = 0.0
-    for n in sorted(set(sizes)):
-        cnt = sizes.count(n)
-        m = sizes.index(n)
-        with T.Session(T.MODEL_COH, n, n, params[m], precision=T.FP32) as s:
-            s.set_state(initial.coh_random_phase(n, n, seed=mem[m]["seed"], k0=mem[m]["k0"]))
+    for key in sorted(set(zip(models, sizes))):
+        cnt = sum(1 for k in zip(models, sizes) if k == key)
+        m = list(zip(models, sizes)).index(key)
+        with T.Session(key[0], key[1], key[1], params[m], precision=T.FP32) as s:
+            s.set_state(member_state(m))
             s.step(T.STEP_AB2, 10)
             seq_ms += cnt * s.time_steps(T.STEP_AB2, 50) / 50
     peak, peak_kind = peaks()
-    S = sum(n * ((n // 2 + 1 + 15) // 16 * 16) * 8 for n in sizes)  # FP32 spectral bytes, all members
-    bytes_step = 68 * S  # (4T + 4F) S per member, T = 14, F = 3, one RHS per AB2 step
+    # FP32 spectral bytes S of each member; (4T + 4F) S per member per AB2 step:
+    # hydro T = 14, F = 3 (68 S); MHD T = 17, F = 6 (92 S)
+    S = [n * ((n // 2 + 1 + 15) // 16 * 16) * 8 for n in sizes]
+    bytes_step = sum((92 if mod == T.MODEL_COM else 68) * s_ for s_, mod in zip(S, models))
     per_s = K / (ms / 1e3)
-    out = {"metric": "ensemble steps/s (256 hydro runs of mixed size, every member one AB2 step)",
+    nhyd = models.count(T.MODEL_COH)
+    kind = f"{nhyd} hydro and {len(mem) - nhyd} MHD" if mixed else "256 hydro"
+    out = {"metric": f"ensemble steps/s ({kind} runs of mixed size, every member one AB2 step)",
            "value": per_s, "unit": "steps/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "256 hydro (*2coh) runs, N in {128,256,384,512} (seeded), nu log-uniform "
-                                  "[1e-4,1e-2], k0 uniform [2,8], FP32, AB2 dt=1e-4",
+           "config": {"workload": (f"{kind} runs (*2coh" + (", *2com" if mixed else "") +
+                                   "), N in {128,256,384,512} (seeded), nu log-uniform [1e-4,1e-2], k0 uniform "
+                                   "[2,8], FP32, AB2 dt=1e-4 hydro" + (", 2e-5 MHD (CS=10, mu=eta=nu)" if mixed
+                                                                       else "")),
                       "sizes": {str(n): sizes.count(n) for n in sorted(set(sizes))}},
            "member_steps_per_s": per_s * len(sizes), "grid_point_steps_per_s": per_s * sum(n * n for n in sizes),
-           "tuning": {"chosen": tuning, "phase_ms": phase_ms, "default_ms_per_step": default_ms},
+           "tuning": {"chosen": tuning, "phase_ms": phase_ms, "default_ms_per_step": default_ms,
+                      "note": "tuning and phase_ms cover the hydro phases"},
            "one_session_per_member_ms_per_step": seq_ms, "speedup_vs_sessions": seq_ms / (ms / K),
            "roofline": {"bound": "hbm", "achieved": bytes_step * per_s / 1e9, "peak": peak, "unit": "GB/s",
                         "frac": bytes_step * per_s / 1e9 / peak, "bytes_per_step": bytes_step,
-                        "note": f"68 S per member per AB2 step, S = FP32 spectral field; peak {peak_kind}"},
-           "gpu_launches": 3 * K}
+                        "note": f"68 S per hydro and 92 S per MHD member per AB2 step, S = FP32 spectral field; "
+                                f"peak {peak_kind}"},
+           "gpu_launches": (3 + (4 if mixed else 0)) * K}
     ens.close()
     print(json.dumps(out), flush=True)
     return 0
@@ -567,8 +593,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=1024, help="grid size (profiling runs only; the metric is at 1024)")
-    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "mhd3d", "kernels", "fft", "mhd4096"],
-                    help="mhd1024: the headline; ensemble: the 256-run batched side workload; "
+    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "ensemble_mixed", "mhd3d", "kernels", "fft", "mhd4096"],
+                    help="mhd1024: the headline; ensemble: the 256-run batched side workload (hydro); "
+                         "ensemble_mixed: the same with every other member an MHD run; "
                          "mhd3d: the 3D path at --grid3^3; kernels: per-kernel times of --model at --grid; "
                          "fft: the engine's 2D transforms against cuFFT; mhd4096: 4096^2 FP32 MHD")
     ap.add_argument("--grid3", type=int, default=256, help="3D grid size of --workload mhd3d")
@@ -582,6 +609,8 @@ def main():
         return run_reference(args)
     if args.workload == "ensemble":
         return run_ensemble(args)
+    if args.workload == "ensemble_mixed":
+        return run_ensemble(args, mixed=True)
     if args.workload == "mhd3d":
         return run_mhd3d(args)
     if args.workload == "kernels":

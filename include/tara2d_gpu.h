@@ -244,8 +244,8 @@ int tara_checkpoint_read(tara_session* s, const char* path, long long* step, dou
 /* ---- learned subgrid closure of the MHD path (no counterpart in the
  * reference) ----
  * A CNN of four periodic 3x3 convolutions (5 -> 32 -> 32 -> 32 -> 4 channels,
- * GELU after the first three; BF16 weights, FP32 activations and
- * accumulation) maps the filtered coarse fields (rho - 1, ux, uy, Bx, By) on
+ * GELU after the first three; BF16 weights, FP32 accumulation; activations
+ * FP32, TF32 into the tensor-core convolutions) maps the filtered coarse fields (rho - 1, ux, uy, Bx, By) on
  * Nc x Nc to the subgrid stress (tau_xx, tau_xy, tau_yy) and EMF, each
  * normalised by the channel means/scales of tara_closure_get_norm.
  * Training pairs are made on the device from an FP64 MHD session on Nf x Nf
@@ -272,6 +272,17 @@ int tara_closure_get_params(tara_closure* c, float* w);
 int tara_closure_set_params(tara_closure* c, const float* w);
 int tara_closure_forward(tara_closure* c, const float* in, int B, float* out);
 int tara_closure_backward(tara_closure* c, const float* in, const float* dout, int B, float* grad);
+/* The 32 -> 32 convolutions (forward and input gradient) run on the tensor
+ * cores (tcgen05 MMAs with TF32 activations, FP32 accumulation in tensor
+ * memory) when on != 0 (the default) and the plane width is a multiple of
+ * 128; on = 0 runs every convolution on CUDA cores with FP32 activations. */
+int tara_closure_set_tensor_cores(tara_closure* c, int on);
+/* TARA_ETIMEOUT if a bounded wait of a tensor-core convolution ran out since
+ * the last check (also reported by forward/backward/train/eval_loss). */
+int tara_closure_status(tara_closure* c);
+/* Device time per call of the network on B samples (ms): forward, and
+ * forward + backward. */
+int tara_closure_time_cnn(tara_closure* c, int B, int reps, float* ms_forward, float* ms_backward);
 int tara_session_attach_closure(tara_session* s, tara_closure* c); /* c = NULL detaches */
 int tara_filter_state(tara_session* fine, tara_session* coarse);
 

@@ -118,6 +118,9 @@ def lib():
         L.tara_closure_set_params.argtypes = [P, P]
         L.tara_closure_forward.argtypes = [P, P, I, P]
         L.tara_closure_backward.argtypes = [P, P, P, I, P]
+        L.tara_closure_set_tensor_cores.argtypes = [P, I]
+        L.tara_closure_status.argtypes = [P]
+        L.tara_closure_time_cnn.argtypes = [P, I, I, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.tara_session_attach_closure.argtypes = [P, P]
         L.tara_filter_state.argtypes = [P, P]
         L.tara_get_state_real.argtypes = [P, PP]
@@ -553,6 +556,16 @@ class Closure:
 
     def __exit__(self, *a):
         self.close()
+
+    def set_tensor_cores(self, on: bool) -> None:
+        """32 -> 32 convolutions on the tensor cores (default) or all on CUDA cores."""
+        check(lib().tara_closure_set_tensor_cores(self._h, int(bool(on))), "tara_closure_set_tensor_cores")
+
+    def time_cnn(self, B: int = 1, reps: int = 20):
+        """Device ms per network call on B samples: (forward, forward + backward)."""
+        f, b = C.c_float(), C.c_float()
+        check(lib().tara_closure_time_cnn(self._h, B, reps, C.byref(f), C.byref(b)), "tara_closure_time_cnn")
+        return f.value, b.value
 
     @staticmethod
     def num_params() -> int:

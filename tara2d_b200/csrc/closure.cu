@@ -415,14 +415,52 @@ int tara_closure_train(tara_closure* c, int first, int count, int epochs, int ba
     TARA_TRY(run_epoch(c, first, count, batch, true, lr, &l));
     if (epoch_loss) epoch_loss[e] = (float)l;
   }
-  return TARA_OK;
+  return c->net.check(c->st);
 }
 int tara_closure_eval_loss(tara_closure* c, int first, int count, float* loss) {
   if (!c || !loss || first < 0 || count < 1 || first + count > c->count) return TARA_EINVAL;
   double l = 0;
   TARA_TRY(run_epoch(c, first, count, c->Bmax, false, 0.0f, &l));
   *loss = (float)l;
+  return c->net.check(c->st);
+}
+int tara_closure_set_tensor_cores(tara_closure* c, int on) {
+  if (!c) return TARA_EINVAL;
+  TARA_CUDA_TRY(cudaStreamSynchronize(c->st));
+  c->net.tensor_cores = on ? 1 : 0;
   return TARA_OK;
+}
+int tara_closure_status(tara_closure* c) { return c ? c->net.check(c->st) : TARA_EINVAL; }
+// device time of `reps` network evaluations on the batch buffer (B samples of
+// whatever it holds): forward alone, and forward + backward with the output
+// gradient in the other batch buffer
+int tara_closure_time_cnn(tara_closure* c, int B, int reps, float* ms_forward, float* ms_backward) {
+  if (!c || !ms_forward || !ms_backward || B < 1 || B > c->Bmax || reps < 1) return TARA_EINVAL;
+  cudaEvent_t e[3];
+  for (auto& x : e) TARA_CUDA_TRY(cudaEventCreate(&x));
+  int r = TARA_OK;
+  r = c->net.forward(c->bin, B, true, c->st);  // warm-up
+  if (r == TARA_OK) r = c->net.backward(c->bin, c->bout, B, c->st);
+  cudaEventRecord(e[0], c->st);
+  for (int k = 0; k < reps && r == TARA_OK; k++) r = c->net.forward(c->bin, B, true, c->st);
+  cudaEventRecord(e[1], c->st);
+  for (int k = 0; k < reps && r == TARA_OK; k++) {
+    r = c->net.forward(c->bin, B, true, c->st);
+    if (r == TARA_OK) r = c->net.backward(c->bin, c->bout, B, c->st);
+  }
+  cudaEventRecord(e[2], c->st);
+  if (cudaEventSynchronize(e[2]) != cudaSuccess && r == TARA_OK) {
+    set_error("cudaEventSynchronize failed");
+    r = TARA_ECUDA;
+  }
+  if (r == TARA_OK) {
+    cudaEventElapsedTime(ms_forward, e[0], e[1]);
+    cudaEventElapsedTime(ms_backward, e[1], e[2]);
+    *ms_forward /= reps;
+    *ms_backward /= reps;
+  }
+  for (auto& x : e) cudaEventDestroy(x);
+  return r == TARA_OK ? c->net.check(c->st) : r;
 }
 int tara_closure_get_params(tara_closure* c, float* w) {
   if (!c || !w) return TARA_EINVAL;
@@ -444,7 +482,7 @@ int tara_closure_forward(tara_closure* c, const float* in, int B, float* out) {
   TARA_TRY(c->net.forward(c->bin, B, true, c->st));
   TARA_CUDA_TRY(cudaMemcpyAsync(out, c->net.out(), (size_t)B * kOut * nc * 4, cudaMemcpyDeviceToHost, c->st));
   TARA_CUDA_TRY(cudaStreamSynchronize(c->st));
-  return TARA_OK;
+  return c->net.check(c->st);
 }
 // gradient of sum(dout * net(in)) with respect to the parameters
 int tara_closure_backward(tara_closure* c, const float* in, const float* dout, int B, float* grad) {
@@ -456,7 +494,7 @@ int tara_closure_backward(tara_closure* c, const float* in, const float* dout, i
   TARA_TRY(c->net.backward(c->bin, c->bout, B, c->st));
   TARA_CUDA_TRY(cudaMemcpyAsync(grad, c->net.grad, cnn_num_params() * 4, cudaMemcpyDeviceToHost, c->st));
   TARA_CUDA_TRY(cudaStreamSynchronize(c->st));
-  return TARA_OK;
+  return c->net.check(c->st);
 }
 int tara_session_attach_closure(tara_session* s, tara_closure* c) {
   if (!s) return TARA_EINVAL;

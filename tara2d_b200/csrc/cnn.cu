@@ -16,6 +16,7 @@
 #include <cstring>
 #include "cnn.cuh"
 #include "plan.h"
+#include "umma.cuh"
 
 namespace tara {
 
@@ -88,6 +89,130 @@ __global__ void __launch_bounds__(256) k_conv(const float* __restrict__ in, cons
     } else {
       out[idx] = v * gelu_d(__ldg(zprev + idx));
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core path of the 32 -> 32 convolutions (the hidden layers forward
+// and their input gradients: 88% of the network's multiply-adds), as an
+// implicit GEMM on tcgen05 (kind::tf32, FP32 accumulation in TMEM).
+//
+// A CTA (four warps) computes kTcRows image rows y0.. of kTcPix pixels
+// x0.. for all 32 output channels: one M = 128 (pixels) x N = 32 (channels)
+// accumulator per row, K = 32 input channels x 9 taps, issued as 9 taps x 4
+// MMAs of K = 8.  The input tile with its one-pixel periodic halo is staged
+// once in shared memory as [channel group of 4][halo row][halo pixel][4]
+// (TF32, rounded to nearest): in the canonical no-swizzle K-major layout
+// every pixel is one 16-byte core-matrix row, so the A operand of tap
+// (dy, dx) is the same buffer with its start shifted by dy halo rows and dx
+// pixels; no im2col copy is made.  Weights are packed once per update as
+// [tap][channel group][cout][4] (the B operand, K-major).  Weights are BF16
+// values, exact in TF32; activations are rounded to TF32 (10-bit mantissa).
+constexpr int kTcRows = 2;                              // image rows per CTA
+constexpr int kTcPix = 128;                             // pixels per row tile (the MMA's M)
+constexpr int kTcXW = kTcPix + 2;                       // halo row width
+constexpr int kTcCG = kCnnHid / 4;                      // channel groups of four TF32 (16 bytes)
+constexpr int kTcAPlane = (kTcRows + 2) * kTcXW;        // halo pixels per channel group
+constexpr size_t kTcABytes = (size_t)kTcCG * kTcAPlane * 16;
+constexpr size_t kTcBBytes = (size_t)9 * kTcCG * kCnnHid * 16;
+constexpr size_t kTcSmem = kTcABytes + kTcBBytes + 16;  // + mbarrier + TMEM address
+constexpr unsigned kTcCols = kCnnHid * kTcRows;         // TMEM columns: one N = 32 accumulator per row
+static_assert(kTcCols >= 32 && (kTcCols & (kTcCols - 1)) == 0, "TMEM allocations are powers of two >= 32");
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1)
+    k_conv_tc(const float* __restrict__ in, const float* __restrict__ wtc, const float* __restrict__ bias,
+              float* __restrict__ z, float* __restrict__ out, const float* __restrict__ zprev, int H, int W,
+              int* __restrict__ status, unsigned long long wait_ns) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float4* As = reinterpret_cast<float4*>(smraw);
+  float4* Bs = reinterpret_cast<float4*>(smraw + kTcABytes);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw + kTcABytes + kTcBBytes);
+  unsigned* slot = reinterpret_cast<unsigned*>(smraw + kTcABytes + kTcBBytes + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int b = blockIdx.z, y0 = blockIdx.y * kTcRows, x0 = blockIdx.x * kTcPix;
+  const size_t plane = (size_t)H * W;
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init_fence();
+  }
+  if (warp == 0) umma::tmem_alloc(slot, kTcCols);
+  // A: halo tile, element (group cg, halo row r, halo pixel px) = channels 4cg..4cg+3
+  const float* inb = in + (size_t)b * kCnnHid * plane;
+  for (int q = tid; q < kTcCG * kTcAPlane; q += 128) {
+    const int cg = q / kTcAPlane, rem = q % kTcAPlane, r = rem / kTcXW, px = rem % kTcXW;
+    const float* src = inb + (size_t)(4 * cg) * plane + (size_t)wrap(y0 + r - 1, H) * W + wrap(x0 + px - 1, W);
+    As[q] = make_float4(umma::to_tf32(__ldg(src)), umma::to_tf32(__ldg(src + plane)),
+                        umma::to_tf32(__ldg(src + 2 * plane)), umma::to_tf32(__ldg(src + 3 * plane)));
+  }
+  // B: packed weights
+  for (int q = tid; q < 9 * kTcCG * kCnnHid; q += 128) Bs[q] = __ldg(reinterpret_cast<const float4*>(wtc) + q);
+  fence_proxy_async_smem();  // the operands are read by the tensor cores (async proxy)
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const unsigned tmem = *slot;
+  if (tid == 0) {
+    constexpr uint32_t idesc = umma::instr_desc(umma::kFmtTF32, kTcPix, kCnnHid);
+    const unsigned a0 = smem_u32(As), b0 = smem_u32(Bs);
+#pragma unroll 1
+    for (int r = 0; r < kTcRows; r++)
+#pragma unroll 1
+      for (int tap = 0; tap < 9; tap++) {
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+        for (int s = 0; s < kTcCG / 2; s++) {  // channel groups 2s, 2s+1: K = 8
+          const unsigned aoff = (unsigned)((2 * s * kTcAPlane + (r + 1 + dy) * kTcXW + 1 + dx) * 16);
+          const unsigned boff = (unsigned)((tap * kTcCG + 2 * s) * kCnnHid * 16);
+          umma::mma_tf32(tmem + (unsigned)(r * kCnnHid), umma::smem_desc(a0 + aoff, kTcAPlane * 16, 128),
+                         umma::smem_desc(b0 + boff, kCnnHid * 16, 128), idesc, tap > 0 || s > 0);
+        }
+      }
+    umma::commit(bar);
+  }
+  const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0, wait_ns));
+  umma::fence_after_sync();
+  if (ok) {
+#pragma unroll 1
+    for (int r = 0; r < kTcRows; r++) {
+      float acc[kCnnHid];
+      umma::ld_32x32b_x32(tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(r * kCnnHid), acc);
+      const size_t po = (size_t)(y0 + r) * W + x0 + 32 * warp + lane;
+#pragma unroll
+      for (int co = 0; co < kCnnHid; co++) {
+        const float v = acc[co] + (bias ? __ldg(bias + co) : 0.0f);
+        const size_t idx = ((size_t)b * kCnnHid + co) * plane + po;
+        if constexpr (EPI == EPI_GELU) {
+          z[idx] = v;
+          out[idx] = gelu(v);
+        } else if constexpr (EPI == EPI_LINEAR) {
+          out[idx] = v;
+        } else {
+          out[idx] = v * gelu_d(__ldg(zprev + idx));
+        }
+      }
+    }
+  } else {
+    // record the failure; give the MMAs in flight a bounded time to finish
+    // before their accumulator is released
+    if (tid == 0) atomicExch(status, TARA_ETIMEOUT);
+    mbar_wait_bounded(bar, 0, wait_ns);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem, kTcCols);
+}
+
+// master W[cout][cin][3][3] of a 32 -> 32 layer -> tensor-core B operands:
+// forward [tap][cin/4][cout][cin%4] and the input-gradient conv's
+// [mirrored tap][cout/4][cin][cout%4], BF16-rounded values as FP32
+__global__ void k_pack_weights_tc(const float* __restrict__ m, float* __restrict__ wf, float* __restrict__ wb) {
+  constexpr int C = kCnnHid, nw = C * C * 9;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x) {
+    const int co = i / (C * 9), ci = (i / 9) % C, tap = i % 9;
+    const float v = __bfloat162float(__float2bfloat16_rn(m[i]));
+    wf[((tap * kTcCG + ci / 4) * C + co) * 4 + ci % 4] = v;
+    wb[(((8 - tap) * kTcCG + co / 4) * C + ci) * 4 + co % 4] = v;
   }
 }
 
@@ -237,6 +362,13 @@ void launch_conv(const float* in, const __nv_bfloat16* w, const float* bias, flo
   }
   launch_conv_split<CIN, COUT, COUT, EPI>(in, w, bias, z, out, zprev, B, H, W, st);
 }
+template <int EPI>
+void launch_conv_tc(const float* in, const float* wtc, const float* bias, float* z, float* out, const float* zprev,
+                    int B, int H, int W, int* status, unsigned long long wait_ns, cudaStream_t st) {
+  auto kern = k_conv_tc<EPI>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+  kern<<<dim3(W / kTcPix, H / kTcRows, B), 128, kTcSmem, st>>>(in, wtc, bias, z, out, zprev, H, W, status, wait_ns);
+}
 template <int CIN, int COUT>
 void launch_dw(const float* in, const float* dz, float* part, float* g, int B, int H, int W, cudaStream_t st) {
   const size_t smem = (size_t)(CIN * (kPlane + 1) + COUT * 256) * sizeof(float);
@@ -250,6 +382,11 @@ void launch_dw(const float* in, const float* dz, float* part, float* g, int B, i
 }  // namespace
 
 int cnn_num_params() { return layer_offset(kCnnLayers); }
+
+bool Cnn::tc_layer(int l) const {
+  const CnnLayerDims d = cnn_layer(l);
+  return tensor_cores && d.cin == kCnnHid && d.cout == kCnnHid && W % kTcPix == 0 && H % kTcRows == 0;
+}
 
 int Cnn::alloc(int H_, int W_, int Bmax_) {
   if (H_ % kTile || W_ % kTile || H_ < kTile || W_ < kTile || Bmax_ < 1) {
@@ -267,7 +404,11 @@ int Cnn::alloc(int H_, int W_, int Bmax_) {
     if (ok && d.gelu) ok = am((void**)&z[l], (size_t)Bmax * d.cout * plane * 4);
     if (ok) ok = am((void**)&a[l], (size_t)Bmax * d.cout * plane * 4);
     bias[l] = biasbuf + layer_offset(l) + d.cout * d.cin * 9;
+    if (ok && d.cin == kCnnHid && d.cout == kCnnHid)
+      ok = am((void**)&wtcf[l], kTcBBytes) && am((void**)&wtcb[l], kTcBBytes);
   }
+  if (ok) ok = am((void**)&status, sizeof(int));
+  if (ok) ok = cudaMemset(status, 0, sizeof(int)) == cudaSuccess;
   for (int k = 0; k < 2 && ok; k++) ok = am((void**)&dz[k], (size_t)Bmax * kCnnHid * plane * 4);
   part_elems = (size_t)Bmax * (H / kTile) * (W / kTile) * (kCnnHid * kCnnHid * 9 + kCnnHid);
   if (ok) ok = am((void**)&part, part_elems * 4);
@@ -285,8 +426,9 @@ void Cnn::release() {
                   (void*)part, (void*)dz[0], (void*)dz[1]})
     if (p) cudaFree(p);
   for (int l = 0; l < kCnnLayers; l++)
-    for (void* p : {(void*)wfwd[l], (void*)wbwd[l], (void*)z[l], (void*)a[l]})
+    for (void* p : {(void*)wfwd[l], (void*)wbwd[l], (void*)z[l], (void*)a[l], (void*)wtcf[l], (void*)wtcb[l]})
       if (p) cudaFree(p);
+  if (status) cudaFree(status);
   *this = Cnn{};
 }
 
@@ -295,6 +437,7 @@ int Cnn::refresh(cudaStream_t st) {
     const CnnLayerDims d = cnn_layer(l);
     k_pack_weights<<<64, 256, 0, st>>>(master + layer_offset(l), d.cin, d.cout, wfwd[l], wbwd[l],
                                        biasbuf + layer_offset(l));
+    if (wtcf[l]) k_pack_weights_tc<<<36, 256, 0, st>>>(master + layer_offset(l), wtcf[l], wtcb[l]);
   }
   TARA_CUDA_TRY(cudaGetLastError());
   return TARA_OK;
@@ -303,8 +446,12 @@ int Cnn::refresh(cudaStream_t st) {
 int Cnn::forward(const float* in, int B, bool, cudaStream_t st) {
   if (B < 1 || B > Bmax) { set_error("batch larger than the CNN buffers"); return TARA_EINVAL; }
   launch_conv<kCnnIn, kCnnHid, EPI_GELU>(in, wfwd[0], bias[0], z[0], a[0], nullptr, B, H, W, st);
-  launch_conv<kCnnHid, kCnnHid, EPI_GELU>(a[0], wfwd[1], bias[1], z[1], a[1], nullptr, B, H, W, st);
-  launch_conv<kCnnHid, kCnnHid, EPI_GELU>(a[1], wfwd[2], bias[2], z[2], a[2], nullptr, B, H, W, st);
+  for (int l = 1; l <= 2; l++) {
+    if (tc_layer(l))
+      launch_conv_tc<EPI_GELU>(a[l - 1], wtcf[l], bias[l], z[l], a[l], nullptr, B, H, W, status, wait_ns, st);
+    else
+      launch_conv<kCnnHid, kCnnHid, EPI_GELU>(a[l - 1], wfwd[l], bias[l], z[l], a[l], nullptr, B, H, W, st);
+  }
   launch_conv<kCnnHid, kCnnOut, EPI_LINEAR>(a[2], wfwd[3], bias[3], nullptr, a[3], nullptr, B, H, W, st);
   TARA_CUDA_TRY(cudaGetLastError());
   return TARA_OK;
@@ -316,12 +463,29 @@ int Cnn::backward(const float* in, const float* dout, int B, cudaStream_t st) {
   launch_dw<kCnnHid, kCnnOut>(a[2], dout, part, grad + layer_offset(3), B, H, W, st);
   launch_conv<kCnnOut, kCnnHid, EPI_GELUGRAD>(dout, wbwd[3], nullptr, nullptr, dz[0], z[2], B, H, W, st);
   launch_dw<kCnnHid, kCnnHid>(a[1], dz[0], part, grad + layer_offset(2), B, H, W, st);
-  launch_conv<kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[0], wbwd[2], nullptr, nullptr, dz[1], z[1], B, H, W, st);
+  if (tc_layer(2))
+    launch_conv_tc<EPI_GELUGRAD>(dz[0], wtcb[2], nullptr, nullptr, dz[1], z[1], B, H, W, status, wait_ns, st);
+  else
+    launch_conv<kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[0], wbwd[2], nullptr, nullptr, dz[1], z[1], B, H, W, st);
   launch_dw<kCnnHid, kCnnHid>(a[0], dz[1], part, grad + layer_offset(1), B, H, W, st);
-  launch_conv<kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[1], wbwd[1], nullptr, nullptr, dz[0], z[0], B, H, W, st);
+  if (tc_layer(1))
+    launch_conv_tc<EPI_GELUGRAD>(dz[1], wtcb[1], nullptr, nullptr, dz[0], z[0], B, H, W, status, wait_ns, st);
+  else
+    launch_conv<kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[1], wbwd[1], nullptr, nullptr, dz[0], z[0], B, H, W, st);
   launch_dw<kCnnIn, kCnnHid>(in, dz[0], part, grad + layer_offset(0), B, H, W, st);
   TARA_CUDA_TRY(cudaGetLastError());
   return TARA_OK;
+}
+
+int Cnn::check(cudaStream_t st) {
+  int v = 0;
+  TARA_CUDA_TRY(cudaMemcpyAsync(&v, status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  TARA_CUDA_TRY(cudaStreamSynchronize(st));
+  if (v != TARA_OK) {
+    TARA_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
+    set_error("a bounded wait of a tensor-core convolution ran out");
+  }
+  return v;
 }
 
 int Cnn::mse(const float* target, int B, cudaStream_t st) {

@@ -1,8 +1,11 @@
 // The closure CNN: 4 periodic 3x3 convolutions, channels
 // 5 -> 32 -> 32 -> 32 -> 4, GELU after the first three.  Weights are kept as
-// FP32 masters (the optimiser's copy) and used rounded to BF16; activations
-// and accumulation are FP32.  Hand-written forward, input-gradient and
-// weight-gradient kernels; Adam on the masters.
+// FP32 masters (the optimiser's copy) and used rounded to BF16; accumulation
+// is FP32.  The 32 -> 32 convolutions (forward and input gradient) run on
+// the tensor cores (tcgen05 MMAs, TF32 activations) unless tensor_cores is
+// 0; the others, and the weight gradients, on CUDA cores with FP32
+// activations.  Hand-written forward, input-gradient and weight-gradient
+// kernels; Adam on the masters.
 //
 // Tensors are [B][C][H][W] FP32 (H, W multiples of 16).  Flat parameter
 // vector: per layer W[cout][cin][3][3] then b[cout].
@@ -39,6 +42,15 @@ struct Cnn {
   float* dz[2] = {};                      // ping-pong gradients w.r.t. pre-activations
   float* part = nullptr;                  // per-CTA weight-gradient partials
   size_t part_elems = 0;
+  // tensor cores (tcgen05, TF32 activations) for the 32 -> 32 convolutions;
+  // 0: every convolution on CUDA cores with FP32 activations (the reference
+  // of the tensor-core path)
+  int tensor_cores = 1;
+  float* wtcf[kCnnLayers] = {};           // tensor-core B operands, forward (32 -> 32 layers)
+  float* wtcb[kCnnLayers] = {};           // and of their input-gradient convolutions
+  int* status = nullptr;                  // device word: TARA_ETIMEOUT when a bounded wait ran out
+  unsigned long long wait_ns = 1000000000ull;
+  bool tc_layer(int l) const;             // layer l's convolutions run on the tensor cores
   double* lossacc = nullptr;
   long long adam_t = 0;
   int alloc(int H, int W, int Bmax);
@@ -53,6 +65,9 @@ struct Cnn {
   // as the output gradient), the loss sum accumulated in lossacc
   int mse(const float* target, int B, cudaStream_t st);
   int adam(float lr, float b1, float b2, float eps, cudaStream_t st);
+  // TARA_ETIMEOUT if a tensor-core kernel's bounded wait ran out since the
+  // last call (synchronises st; clears the word)
+  int check(cudaStream_t st);
   float* out() const { return a[kCnnLayers - 1]; }
 };
 
