@@ -295,7 +295,8 @@ int run_epoch(tara_closure* c, int first, int count, int batch, bool train, floa
     TARA_CUDA_TRY(cudaStreamSynchronize(c->st));  // pick[] is reused by the next batch
   }
   double acc = 0.0;
-  TARA_CUDA_TRY(cudaMemcpy(&acc, c->net.lossacc, sizeof(double), cudaMemcpyDeviceToHost));
+  TARA_CUDA_TRY(cudaMemcpyAsync(&acc, c->net.lossacc, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  TARA_CUDA_TRY(cudaStreamSynchronize(c->st));
   // k_mse sums squared errors of each batch; report the mean over all elements
   *loss = acc / ((double)count * kOut * N * N);
   return TARA_OK;
@@ -342,7 +343,10 @@ int tara_closure_open(tara_closure** out, int Nc, int capacity, int batch_max, u
     for (int k = 0; k < d.cout * d.cin * 9; k++) w[off + k] = sd * nd(c->rng);
     off += d.cout * d.cin * 9 + d.cout;
   }
-  TARA_CUDA_TRY(cudaMemcpy(c->net.master, w.data(), np * 4, cudaMemcpyHostToDevice));
+  // every copy of the closure is ordered on its (non-blocking) stream: a plain
+  // cudaMemcpy from pageable memory may return before the data has reached
+  // the device, and the weight packing on c->st could then read old weights
+  TARA_CUDA_TRY(cudaMemcpyAsync(c->net.master, w.data(), np * 4, cudaMemcpyHostToDevice, c->st));
   TARA_TRY(c->net.refresh(c->st));
   for (int k = 0; k < kIn; k++) { c->norm.mi[k] = 0.0f; c->norm.si[k] = 1.0f; }
   for (int k = 0; k < kOut; k++) { c->norm.mo[k] = 0.0f; c->norm.so[k] = 1.0f; }
@@ -364,8 +368,10 @@ int tara_closure_add_pair(tara_closure* c, tara_session* fine) {
 int tara_closure_get_pair(tara_closure* c, int idx, float* in5, float* out4) {
   if (!c || idx < 0 || idx >= c->count || !in5 || !out4) return TARA_EINVAL;
   const size_t nc = (size_t)c->Nc * c->Nc;
-  TARA_CUDA_TRY(cudaMemcpy(in5, c->din + (size_t)idx * kIn * nc, kIn * nc * 4, cudaMemcpyDeviceToHost));
-  TARA_CUDA_TRY(cudaMemcpy(out4, c->dout + (size_t)idx * kOut * nc, kOut * nc * 4, cudaMemcpyDeviceToHost));
+  TARA_CUDA_TRY(cudaMemcpyAsync(in5, c->din + (size_t)idx * kIn * nc, kIn * nc * 4, cudaMemcpyDeviceToHost, c->st));
+  TARA_CUDA_TRY(
+      cudaMemcpyAsync(out4, c->dout + (size_t)idx * kOut * nc, kOut * nc * 4, cudaMemcpyDeviceToHost, c->st));
+  TARA_CUDA_TRY(cudaStreamSynchronize(c->st));
   return TARA_OK;
 }
 // norm: mean_in[5], std_in[5], mean_out[4], std_out[4]
@@ -464,12 +470,13 @@ int tara_closure_time_cnn(tara_closure* c, int B, int reps, float* ms_forward, f
 }
 int tara_closure_get_params(tara_closure* c, float* w) {
   if (!c || !w) return TARA_EINVAL;
-  TARA_CUDA_TRY(cudaMemcpy(w, c->net.master, cnn_num_params() * 4, cudaMemcpyDeviceToHost));
+  TARA_CUDA_TRY(cudaMemcpyAsync(w, c->net.master, cnn_num_params() * 4, cudaMemcpyDeviceToHost, c->st));
+  TARA_CUDA_TRY(cudaStreamSynchronize(c->st));
   return TARA_OK;
 }
 int tara_closure_set_params(tara_closure* c, const float* w) {
   if (!c || !w) return TARA_EINVAL;
-  TARA_CUDA_TRY(cudaMemcpy(c->net.master, w, cnn_num_params() * 4, cudaMemcpyHostToDevice));
+  TARA_CUDA_TRY(cudaMemcpyAsync(c->net.master, w, cnn_num_params() * 4, cudaMemcpyHostToDevice, c->st));
   TARA_TRY(c->net.refresh(c->st));
   TARA_CUDA_TRY(cudaStreamSynchronize(c->st));
   return TARA_OK;

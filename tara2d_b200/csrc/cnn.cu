@@ -12,6 +12,7 @@
 //               (cout, cin) pairs and all 9 taps; per-CTA partials are then
 //               summed in a fixed order by k_sum_parts.
 //   k_mse, k_adam, k_pack_weights: loss/gradient, optimiser, BF16 layouts.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include "cnn.cuh"
@@ -115,92 +116,135 @@ constexpr int kTcCG = kCnnHid / 4;                      // channel groups of fou
 constexpr int kTcAPlane = (kTcRows + 2) * kTcXW;        // halo pixels per channel group
 constexpr size_t kTcABytes = (size_t)kTcCG * kTcAPlane * 16;
 constexpr size_t kTcBBytes = (size_t)9 * kTcCG * kCnnHid * 16;
-constexpr size_t kTcSmem = kTcABytes + kTcBBytes + 16;  // + mbarrier + TMEM address
+constexpr size_t kTcSmem = kTcABytes + kTcBBytes + 32;  // + 2 mbarriers, TMEM address, issue flag
 constexpr unsigned kTcCols = kCnnHid * kTcRows;         // TMEM columns: one N = 32 accumulator per row
 static_assert(kTcCols >= 32 && (kTcCols & (kTcCols - 1)) == 0, "TMEM allocations are powers of two >= 32");
 
 template <int EPI>
 __global__ void __launch_bounds__(128, 1)
     k_conv_tc(const float* __restrict__ in, const float* __restrict__ wtc, const float* __restrict__ bias,
-              float* __restrict__ z, float* __restrict__ out, const float* __restrict__ zprev, int H, int W,
+              float* __restrict__ z, float* __restrict__ out, const float* __restrict__ zprev, int B, int H, int W,
               int* __restrict__ status, unsigned long long wait_ns) {
   extern __shared__ __align__(128) unsigned char smraw[];
   float4* As = reinterpret_cast<float4*>(smraw);
   float4* Bs = reinterpret_cast<float4*>(smraw + kTcABytes);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw + kTcABytes + kTcBBytes);
-  unsigned* slot = reinterpret_cast<unsigned*>(smraw + kTcABytes + kTcBBytes + 8);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + kTcABytes + kTcBBytes);  // [0] weights, [1] MMAs
+  unsigned* slot = reinterpret_cast<unsigned*>(smraw + kTcABytes + kTcBBytes + 16);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int b = blockIdx.z, y0 = blockIdx.y * kTcRows, x0 = blockIdx.x * kTcPix;
   const size_t plane = (size_t)H * W;
+  const int tx = W / kTcPix, ty = H / kTcRows, ntiles = tx * ty * B;
   if (tid == 0) {
-    mbar_init(bar, 1);
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
     mbar_init_fence();
+    // the weights (B operand) once per CTA: one bulk copy, overlapping the first tile's staging
+    mbar_expect_tx(&bars[0], (unsigned)kTcBBytes);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(Bs)),
+                 "l"(wtc), "r"((unsigned)kTcBBytes), "r"(smem_u32(&bars[0]))
+                 : "memory");
   }
   if (warp == 0) umma::tmem_alloc(slot, kTcCols);
-  // A: halo tile, element (group cg, halo row r, halo pixel px) = channels 4cg..4cg+3
-  const float* inb = in + (size_t)b * kCnnHid * plane;
-  for (int q = tid; q < kTcCG * kTcAPlane; q += 128) {
-    const int cg = q / kTcAPlane, rem = q % kTcAPlane, r = rem / kTcXW, px = rem % kTcXW;
-    const float* src = inb + (size_t)(4 * cg) * plane + (size_t)wrap(y0 + r - 1, H) * W + wrap(x0 + px - 1, W);
-    As[q] = make_float4(umma::to_tf32(__ldg(src)), umma::to_tf32(__ldg(src + plane)),
-                        umma::to_tf32(__ldg(src + 2 * plane)), umma::to_tf32(__ldg(src + 3 * plane)));
-  }
-  // B: packed weights
-  for (int q = tid; q < 9 * kTcCG * kCnnHid; q += 128) Bs[q] = __ldg(reinterpret_cast<const float4*>(wtc) + q);
-  fence_proxy_async_smem();  // the operands are read by the tensor cores (async proxy)
-  umma::fence_before_sync();
-  __syncthreads();
-  umma::fence_after_sync();
-  const unsigned tmem = *slot;
-  if (tid == 0) {
-    constexpr uint32_t idesc = umma::instr_desc(umma::kFmtTF32, kTcPix, kCnnHid);
-    const unsigned a0 = smem_u32(As), b0 = smem_u32(Bs);
+  bool ok = true;
+  int it = 0;
 #pragma unroll 1
-    for (int r = 0; r < kTcRows; r++)
-#pragma unroll 1
-      for (int tap = 0; tap < 9; tap++) {
-        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, it++) {
+    const int b = tile / (tx * ty), rem_t = tile % (tx * ty);
+    const int y0 = (rem_t / tx) * kTcRows, x0 = (rem_t % tx) * kTcPix;
+    const float* inb = in + (size_t)b * kCnnHid * plane;
+    // A: halo tile [cg][halo row][halo pixel][4 channels]; the 128 interior
+    // pixels of a row by 16-byte loads along x (4 pixels of each of 4 channels)
+    for (int q = tid; q < kTcCG * (kTcRows + 2) * (kTcPix / 4); q += 128) {
+      const int k4 = q % (kTcPix / 4), rr = q / (kTcPix / 4), r = rr % (kTcRows + 2), cg = rr / (kTcRows + 2);
+      const float* src = inb + (size_t)(4 * cg) * plane + (size_t)wrap(y0 + r - 1, H) * W + x0 + 4 * k4;
+      float4 c[4];
 #pragma unroll
-        for (int s = 0; s < kTcCG / 2; s++) {  // channel groups 2s, 2s+1: K = 8
-          const unsigned aoff = (unsigned)((2 * s * kTcAPlane + (r + 1 + dy) * kTcXW + 1 + dx) * 16);
-          const unsigned boff = (unsigned)((tap * kTcCG + 2 * s) * kCnnHid * 16);
-          umma::mma_tf32(tmem + (unsigned)(r * kCnnHid), umma::smem_desc(a0 + aoff, kTcAPlane * 16, 128),
-                         umma::smem_desc(b0 + boff, kCnnHid * 16, 128), idesc, tap > 0 || s > 0);
-        }
-      }
-    umma::commit(bar);
-  }
-  const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0, wait_ns));
-  umma::fence_after_sync();
-  if (ok) {
-#pragma unroll 1
-    for (int r = 0; r < kTcRows; r++) {
-      float acc[kCnnHid];
-      umma::ld_32x32b_x32(tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(r * kCnnHid), acc);
-      const size_t po = (size_t)(y0 + r) * W + x0 + 32 * warp + lane;
-#pragma unroll
-      for (int co = 0; co < kCnnHid; co++) {
-        const float v = acc[co] + (bias ? __ldg(bias + co) : 0.0f);
-        const size_t idx = ((size_t)b * kCnnHid + co) * plane + po;
-        if constexpr (EPI == EPI_GELU) {
-          z[idx] = v;
-          out[idx] = gelu(v);
-        } else if constexpr (EPI == EPI_LINEAR) {
-          out[idx] = v;
-        } else {
-          out[idx] = v * gelu_d(__ldg(zprev + idx));
-        }
-      }
+      for (int j = 0; j < 4; j++) c[j] = __ldg(reinterpret_cast<const float4*>(src + j * plane));
+      float4* dst = As + (size_t)(cg * (kTcRows + 2) + r) * kTcXW + 1 + 4 * k4;
+      dst[0] = make_float4(umma::to_tf32(c[0].x), umma::to_tf32(c[1].x), umma::to_tf32(c[2].x), umma::to_tf32(c[3].x));
+      dst[1] = make_float4(umma::to_tf32(c[0].y), umma::to_tf32(c[1].y), umma::to_tf32(c[2].y), umma::to_tf32(c[3].y));
+      dst[2] = make_float4(umma::to_tf32(c[0].z), umma::to_tf32(c[1].z), umma::to_tf32(c[2].z), umma::to_tf32(c[3].z));
+      dst[3] = make_float4(umma::to_tf32(c[0].w), umma::to_tf32(c[1].w), umma::to_tf32(c[2].w), umma::to_tf32(c[3].w));
     }
-  } else {
-    // record the failure; give the MMAs in flight a bounded time to finish
-    // before their accumulator is released
-    if (tid == 0) atomicExch(status, TARA_ETIMEOUT);
-    mbar_wait_bounded(bar, 0, wait_ns);
+    // the two halo pixels of every row (periodic wrap in x)
+    for (int q = tid; q < kTcCG * (kTcRows + 2) * 2; q += 128) {
+      const int side = q & 1, rr = q >> 1, r = rr % (kTcRows + 2), cg = rr / (kTcRows + 2);
+      const int px = side ? kTcXW - 1 : 0;
+      const float* src =
+          inb + (size_t)(4 * cg) * plane + (size_t)wrap(y0 + r - 1, H) * W + wrap(x0 + px - 1, W);
+      As[(size_t)(cg * (kTcRows + 2) + r) * kTcXW + px] =
+          make_float4(umma::to_tf32(__ldg(src)), umma::to_tf32(__ldg(src + plane)),
+                      umma::to_tf32(__ldg(src + 2 * plane)), umma::to_tf32(__ldg(src + 3 * plane)));
+    }
+    fence_proxy_async_smem();  // the operands are read by the tensor cores (async proxy)
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const unsigned tmem = *slot;
+    if (tid == 0) {
+      bool wok = it > 0 || mbar_wait_bounded(&bars[0], 0, wait_ns);
+      if (wok) {
+        constexpr uint32_t idesc = umma::instr_desc(umma::kFmtTF32, kTcPix, kCnnHid);
+        const unsigned a0 = smem_u32(As), b0 = smem_u32(Bs);
+#pragma unroll 1
+        for (int r = 0; r < kTcRows; r++)
+#pragma unroll 1
+          for (int tap = 0; tap < 9; tap++) {
+            const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+            for (int s = 0; s < kTcCG / 2; s++) {  // channel groups 2s, 2s+1: K = 8
+              const unsigned aoff = (unsigned)((2 * s * kTcAPlane + (r + 1 + dy) * kTcXW + 1 + dx) * 16);
+              const unsigned boff = (unsigned)((tap * kTcCG + 2 * s) * kCnnHid * 16);
+              umma::mma_tf32(tmem + (unsigned)(r * kCnnHid), umma::smem_desc(a0 + aoff, kTcAPlane * 16, 128),
+                             umma::smem_desc(b0 + boff, kCnnHid * 16, 128), idesc, tap > 0 || s > 0);
+            }
+          }
+        umma::commit(&bars[1]);
+      } else {
+        atomicExch(status, TARA_ETIMEOUT);
+      }
+      slot[1] = wok ? 1u : 0u;
+    }
+    __syncthreads();
+    ok = slot[1] != 0;
+    if (ok) ok = __syncthreads_and(mbar_wait_bounded(&bars[1], it & 1, wait_ns));
+    umma::fence_after_sync();
+    if (ok) {
+#pragma unroll 1
+      for (int r = 0; r < kTcRows; r++) {
+        float acc[kCnnHid];
+        umma::ld_32x32b_x32(tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(r * kCnnHid), acc);
+        const size_t po = (size_t)(y0 + r) * W + x0 + 32 * warp + lane;
+#pragma unroll
+        for (int co = 0; co < kCnnHid; co++) {
+          const float v = acc[co] + (bias ? __ldg(bias + co) : 0.0f);
+          const size_t idx = ((size_t)b * kCnnHid + co) * plane + po;
+          if constexpr (EPI == EPI_GELU) {
+            z[idx] = v;
+            out[idx] = gelu(v);
+          } else if constexpr (EPI == EPI_LINEAR) {
+            out[idx] = v;
+          } else {
+            out[idx] = v * gelu_d(__ldg(zprev + idx));
+          }
+        }
+      }
+    } else if (slot[1]) {
+      // the MMAs were issued but did not complete in time: record it and give
+      // them a bounded time to finish before their accumulator is released
+      if (tid == 0) atomicExch(status, TARA_ETIMEOUT);
+      mbar_wait_bounded(&bars[1], it & 1, wait_ns);
+    }
+    umma::fence_before_sync();
+    __syncthreads();  // the accumulator and the A tile are free again
   }
-  umma::fence_before_sync();
-  __syncthreads();
-  if (warp == 0) umma::tmem_dealloc(tmem, kTcCols);
+  if (it == 0 || !ok) {
+    // the weight copy may still be in flight (no tile, or a failed wait):
+    // let it land before the CTA's shared memory is released
+    if (tid == 0) mbar_wait_bounded(&bars[0], 0, wait_ns);
+    __syncthreads();
+  }
+  if (warp == 0) umma::tmem_dealloc(*slot, kTcCols);
 }
 
 // master W[cout][cin][3][3] of a 32 -> 32 layer -> tensor-core B operands:
@@ -367,7 +411,14 @@ void launch_conv_tc(const float* in, const float* wtc, const float* bias, float*
                     int B, int H, int W, int* status, unsigned long long wait_ns, cudaStream_t st) {
   auto kern = k_conv_tc<EPI>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
-  kern<<<dim3(W / kTcPix, H / kTcRows, B), 128, kTcSmem, st>>>(in, wtc, bias, z, out, zprev, H, W, status, wait_ns);
+  // persistent: at most as many CTAs as fit, each loading the weights once
+  int per_sm = 1, dev = 0, sms = 148;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, kTcSmem);
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int ntiles = (W / kTcPix) * (H / kTcRows) * B;
+  const int grid = std::min(ntiles, std::max(per_sm, 1) * sms);
+  kern<<<grid, 128, kTcSmem, st>>>(in, wtc, bias, z, out, zprev, B, H, W, status, wait_ns);
 }
 template <int CIN, int COUT>
 void launch_dw(const float* in, const float* dz, float* part, float* g, int B, int H, int W, cudaStream_t st) {
@@ -418,6 +469,9 @@ int Cnn::alloc(int H_, int W_, int Bmax_) {
   }
   cudaMemset(adam_m, 0, np * 4);
   cudaMemset(adam_v, 0, np * 4);
+  // the memsets run on the legacy stream, which the closure's non-blocking
+  // stream does not wait for: finish them here
+  TARA_CUDA_TRY(cudaDeviceSynchronize());
   return TARA_OK;
 }
 

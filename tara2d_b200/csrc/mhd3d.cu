@@ -671,7 +671,11 @@ struct tara3d {
       set_error("cudaMalloc of the 3D tables failed");
       return TARA_ENOMEM;
     }
-    TARA_CUDA_TRY(cudaMemcpy(tables, h.data(), total, cudaMemcpyHostToDevice));
+    // on the session's (non-blocking) stream and waited for: a plain copy from
+    // pageable memory may return before the data reaches the device and is
+    // not ordered with that stream's kernels
+    TARA_CUDA_TRY(cudaMemcpyAsync(tables, h.data(), total, cudaMemcpyHostToDevice, st));
+    TARA_CUDA_TRY(cudaStreamSynchronize(st));
     char* b = (char*)tables;
     twy = (const Cx<double>*)(b + o_ty);
     twz = (const Cx<double>*)(b + o_tz);

@@ -43,14 +43,19 @@ __host__ __device__ constexpr uint32_t instr_desc(unsigned fmt, int M, int N) {
 constexpr unsigned kFmtTF32 = 2;
 
 // TMEM allocation of ncols columns (a power of two >= 32) by one whole warp;
-// the address is written to the shared-memory word `slot`.
+// the address is written to the shared-memory word `slot`.  The
+// instruction is warp-collective (.sync.aligned): the warp is reconverged
+// first, since a lane may arrive from a branch only it took (without this,
+// results were wrong intermittently on the GPU).
 __device__ __forceinline__ void tmem_alloc(unsigned* slot, unsigned ncols) {
+  __syncwarp();
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
                "r"(ncols)
                : "memory");
   asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
 }
 __device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
+  __syncwarp();
   asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
