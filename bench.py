@@ -583,6 +583,53 @@ class Ranks:
 
 
 # ------------------------------------------------------------------ our arm
+def run_closure(args):
+    """Side workload: the cost of the learned closure in the 256^2 coarse MHD
+    run (FP64, RK4, dt = 1e-4, nu = eta = 1e-4, random-phase state with
+    k0 = 4): device ms per RK4 step without a closure, with the closure's
+    network on tensor cores, and with it on CUDA cores; plus the network's own
+    device time per 256^2 field (forward; forward + backward).  The network's
+    parameters are seeded random values (the cost does not depend on them)."""
+    import numpy as np
+    import tara2d_b200 as T
+    from tara2d_b200 import initial
+    N = 256
+    kw = dict(Lx=2 * PI, Ly=2 * PI, pi=PI, dt=1e-4, mu=1e-4, eta=1e-4, CS=100.0, spheat=5.0 / 3.0, ms=1.0,
+              mu_0=1.0, kf=1.0, A=0.0, fix_curlB=0)
+    st = initial.com_random_phase(N, N, seed=3, k0=4.0)
+    W, K = max(3, args.warmup), max(10, args.steps)
+    rng = np.random.default_rng(0)
+    w = (0.02 * rng.standard_normal(T.Closure.num_params())).astype(np.float32)
+    res = {}
+    with T.Closure(N, 1, batch_max=1) as c:
+        c.set_params(w)
+        res["cnn_tc_ms"] = c.time_cnn(1, 20)
+        c.set_tensor_cores(False)
+        res["cnn_cuda_ms"] = c.time_cnn(1, 20)
+        for mode in ("none", "tensor_cores", "cuda_cores"):
+            with T.Session(T.MODEL_COM, N, N, T.Params.make(**kw)) as s:
+                s.set_state(st)
+                if mode != "none":
+                    c.set_tensor_cores(mode == "tensor_cores")
+                    T.attach_closure(s, c)
+                s.step(T.STEP_RK4, W)
+                res[mode] = s.time_steps(T.STEP_RK4, K) / K
+    out = {"metric": "closure cost: ms per RK4 step of the 256^2 coarse MHD run (FP64)",
+           "value": res["tensor_cores"], "unit": "ms/step", "n_gpus": 1, "steps": K, "warmup": W,
+           "higher_is_better": False, "dtype": "f64 solver, tf32/f32 network", "data": "synthetic",
+           "config": {"workload": "256^2 MHD RK4 dt=1e-4 nu=eta=1e-4, random-phase k0=4; closure CNN "
+                                  "5->32->32->32->4 (3x3, GELU), seeded random parameters"},
+           "unclosed_ms_per_step": res["none"], "closed_tensor_cores_ms_per_step": res["tensor_cores"],
+           "closed_cuda_cores_ms_per_step": res["cuda_cores"],
+           "closed_over_unclosed": {"tensor_cores": res["tensor_cores"] / res["none"],
+                                    "cuda_cores": res["cuda_cores"] / res["none"]},
+           "cnn_ms_per_field": {"tensor_cores": {"forward": res["cnn_tc_ms"][0], "forward_backward": res["cnn_tc_ms"][1]},
+                                "cuda_cores": {"forward": res["cnn_cuda_ms"][0],
+                                               "forward_backward": res["cnn_cuda_ms"][1]}}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -593,11 +640,12 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=1024, help="grid size (profiling runs only; the metric is at 1024)")
-    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "ensemble_mixed", "mhd3d", "kernels", "fft", "mhd4096"],
+    ap.add_argument("--workload", default="mhd1024", choices=["mhd1024", "ensemble", "ensemble_mixed", "mhd3d", "kernels", "fft", "mhd4096", "closure"],
                     help="mhd1024: the headline; ensemble: the 256-run batched side workload (hydro); "
                          "ensemble_mixed: the same with every other member an MHD run; "
                          "mhd3d: the 3D path at --grid3^3; kernels: per-kernel times of --model at --grid; "
-                         "fft: the engine's 2D transforms against cuFFT; mhd4096: 4096^2 FP32 MHD")
+                         "fft: the engine's 2D transforms against cuFFT; mhd4096: 4096^2 FP32 MHD; "
+                         "closure: the learned closure's cost in the 256^2 coarse run")
     ap.add_argument("--grid3", type=int, default=256, help="3D grid size of --workload mhd3d")
     ap.add_argument("--model", choices=["com", "coh", "csh", "css"], default="com", help="--workload kernels")
     ap.add_argument("--fp32", action="store_true", help="--workload kernels: FP32 session")
@@ -617,6 +665,8 @@ def main():
         return run_kernels(args)
     if args.workload == "fft":
         return run_fft(args)
+    if args.workload == "closure":
+        return run_closure(args)
     if args.workload == "mhd4096":
         return run_mhd4096(args)
 

@@ -94,87 +94,107 @@ __global__ void __launch_bounds__(256) k_conv(const float* __restrict__ in, cons
 }
 
 // ---------------------------------------------------------------------------
-// Tensor-core path of the 32 -> 32 convolutions (the hidden layers forward
-// and their input gradients: 88% of the network's multiply-adds), as an
-// implicit GEMM on tcgen05 (kind::tf32, FP32 accumulation in TMEM).
+// Tensor-core path of the convolutions (all four layers forward and the
+// three input-gradient convolutions), as an implicit GEMM on tcgen05
+// (kind::tf32, FP32 accumulation in TMEM).
 //
-// A CTA (four warps) computes kTcRows image rows y0.. of kTcPix pixels
-// x0.. for all 32 output channels: one M = 128 (pixels) x N = 32 (channels)
-// accumulator per row, K = 32 input channels x 9 taps, issued as 9 taps x 4
-// MMAs of K = 8.  The input tile with its one-pixel periodic halo is staged
-// once in shared memory as [channel group of 4][halo row][halo pixel][4]
-// (TF32, rounded to nearest): in the canonical no-swizzle K-major layout
-// every pixel is one 16-byte core-matrix row, so the A operand of tap
-// (dy, dx) is the same buffer with its start shifted by dy halo rows and dx
-// pixels; no im2col copy is made.  Weights are packed once per update as
-// [tap][channel group][cout][4] (the B operand, K-major).  Weights are BF16
-// values, exact in TF32; activations are rounded to TF32 (10-bit mantissa).
-constexpr int kTcRows = 2;                              // image rows per CTA
-constexpr int kTcPix = 128;                             // pixels per row tile (the MMA's M)
+// A CTA (four warps) computes one image row y0 of kTcPix pixels x0.. for
+// all output channels of a layer: one M = 128 (pixels) x N accumulator,
+// K = (input channels) x 9 taps, issued as 9 taps x CG/2 MMAs of K = 8.  The
+// input row with its one-pixel periodic halo (three image rows) is staged in
+// shared memory as [channel group of 4][halo row][halo pixel][4] (TF32,
+// rounded to nearest): in the canonical no-swizzle K-major layout every pixel
+// is one 16-byte core-matrix row, so the A operand of tap (dy, dx) is the
+// same buffer with its start shifted by dy halo rows and dx pixels; no
+// im2col copy is made.  Weights are packed once per update as
+// [tap][channel group][N][4] (the B operand, K-major), zero where a layer has
+// fewer channels than the padded shape: 5 input channels are two groups
+// (channels 5..7 zero), 4 input channels are two groups (one zero), 4 output
+// channels are an N = 16 tile.  Weights are BF16 values, exact in TF32;
+// activations are rounded to TF32 (10-bit mantissa).
+constexpr int kTcPix = 128;                             // pixels per tile (the MMA's M)
 constexpr int kTcXW = kTcPix + 2;                       // halo row width
-constexpr int kTcCG = kCnnHid / 4;                      // channel groups of four TF32 (16 bytes)
-constexpr int kTcAPlane = (kTcRows + 2) * kTcXW;        // halo pixels per channel group
-constexpr size_t kTcABytes = (size_t)kTcCG * kTcAPlane * 16;
-constexpr size_t kTcBBytes = (size_t)9 * kTcCG * kCnnHid * 16;
-constexpr size_t kTcSmem = kTcABytes + kTcBBytes + 32;  // + 2 mbarriers, TMEM address, issue flag
-constexpr unsigned kTcCols = kCnnHid * kTcRows;         // TMEM columns: one N = 32 accumulator per row
-static_assert(kTcCols >= 32 && (kTcCols & (kTcCols - 1)) == 0, "TMEM allocations are powers of two >= 32");
+constexpr int kTcAPlane = 3 * kTcXW;                    // halo pixels per channel group (3 rows)
+constexpr unsigned kTcCols = 32;                        // TMEM columns (N <= 32)
 
-template <int EPI>
+// Shared-memory geometry of a layer shape: CG channel groups of four
+// (even: one MMA covers two), N accumulator columns.
+template <int CG, int NN> struct TcGeom {
+  static_assert(CG % 2 == 0 && (NN == 16 || NN == 32), "padded layer shape");
+  static constexpr size_t A_BYTES = (size_t)CG * kTcAPlane * 16;
+  static constexpr size_t B_BYTES = (size_t)9 * CG * NN * 16;
+  static constexpr size_t SMEM = A_BYTES + B_BYTES + 32;  // + 2 mbarriers, TMEM address, issue flag
+};
+
+// Input [B][CINR][H][W] -> output [B][COUT][H][W] (and z for GELU); wtc: the
+// packed B operand [9][CG][NN][4].
+template <int CG, int NN, int COUT, int CINR, int EPI>
 __global__ void __launch_bounds__(128, 1)
     k_conv_tc(const float* __restrict__ in, const float* __restrict__ wtc, const float* __restrict__ bias,
               float* __restrict__ z, float* __restrict__ out, const float* __restrict__ zprev, int B, int H, int W,
               int* __restrict__ status, unsigned long long wait_ns) {
+  using G = TcGeom<CG, NN>;
+  static_assert(CINR <= 4 * CG && COUT <= NN, "layer does not fit the padded shape");
   extern __shared__ __align__(128) unsigned char smraw[];
   float4* As = reinterpret_cast<float4*>(smraw);
-  float4* Bs = reinterpret_cast<float4*>(smraw + kTcABytes);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + kTcABytes + kTcBBytes);  // [0] weights, [1] MMAs
-  unsigned* slot = reinterpret_cast<unsigned*>(smraw + kTcABytes + kTcBBytes + 16);
+  float4* Bs = reinterpret_cast<float4*>(smraw + G::A_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smraw + G::A_BYTES + G::B_BYTES);  // [0] weights, [1] MMAs
+  unsigned* slot = reinterpret_cast<unsigned*>(smraw + G::A_BYTES + G::B_BYTES + 16);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const size_t plane = (size_t)H * W;
-  const int tx = W / kTcPix, ty = H / kTcRows, ntiles = tx * ty * B;
+  const int tx = W / kTcPix, ntiles = tx * H * B;
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     mbar_init_fence();
     // the weights (B operand) once per CTA: one bulk copy, overlapping the first tile's staging
-    mbar_expect_tx(&bars[0], (unsigned)kTcBBytes);
+    mbar_expect_tx(&bars[0], (unsigned)G::B_BYTES);
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_u32(Bs)),
-                 "l"(wtc), "r"((unsigned)kTcBBytes), "r"(smem_u32(&bars[0]))
+                 "l"(wtc), "r"((unsigned)G::B_BYTES), "r"(smem_u32(&bars[0]))
                  : "memory");
   }
   if (warp == 0) umma::tmem_alloc(slot, kTcCols);
+  // channel c of a group: 4 values of one pixel (zero past the layer's channels)
+  auto chan = [&](const float* src, int c0, int j) -> float {
+    if constexpr (CINR == 4 * CG) return umma::to_tf32(__ldg(src + (size_t)j * plane));
+    else return c0 + j < CINR ? umma::to_tf32(__ldg(src + (size_t)j * plane)) : 0.0f;
+  };
   bool ok = true;
   int it = 0;
 #pragma unroll 1
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, it++) {
-    const int b = tile / (tx * ty), rem_t = tile % (tx * ty);
-    const int y0 = (rem_t / tx) * kTcRows, x0 = (rem_t % tx) * kTcPix;
-    const float* inb = in + (size_t)b * kCnnHid * plane;
+    const int b = tile / (tx * H), rem_t = tile % (tx * H);
+    const int y0 = rem_t / tx, x0 = (rem_t % tx) * kTcPix;
+    const float* inb = in + (size_t)b * CINR * plane;
     // A: halo tile [cg][halo row][halo pixel][4 channels]; the 128 interior
-    // pixels of a row by 16-byte loads along x (4 pixels of each of 4 channels)
-    for (int q = tid; q < kTcCG * (kTcRows + 2) * (kTcPix / 4); q += 128) {
-      const int k4 = q % (kTcPix / 4), rr = q / (kTcPix / 4), r = rr % (kTcRows + 2), cg = rr / (kTcRows + 2);
+    // pixels of a row by 16-byte loads along x (4 pixels of each channel)
+    for (int q = tid; q < CG * 3 * (kTcPix / 4); q += 128) {
+      const int k4 = q % (kTcPix / 4), rr = q / (kTcPix / 4), r = rr % 3, cg = rr / 3;
       const float* src = inb + (size_t)(4 * cg) * plane + (size_t)wrap(y0 + r - 1, H) * W + x0 + 4 * k4;
       float4 c[4];
 #pragma unroll
-      for (int j = 0; j < 4; j++) c[j] = __ldg(reinterpret_cast<const float4*>(src + j * plane));
-      float4* dst = As + (size_t)(cg * (kTcRows + 2) + r) * kTcXW + 1 + 4 * k4;
-      dst[0] = make_float4(umma::to_tf32(c[0].x), umma::to_tf32(c[1].x), umma::to_tf32(c[2].x), umma::to_tf32(c[3].x));
-      dst[1] = make_float4(umma::to_tf32(c[0].y), umma::to_tf32(c[1].y), umma::to_tf32(c[2].y), umma::to_tf32(c[3].y));
-      dst[2] = make_float4(umma::to_tf32(c[0].z), umma::to_tf32(c[1].z), umma::to_tf32(c[2].z), umma::to_tf32(c[3].z));
-      dst[3] = make_float4(umma::to_tf32(c[0].w), umma::to_tf32(c[1].w), umma::to_tf32(c[2].w), umma::to_tf32(c[3].w));
+      for (int j = 0; j < 4; j++) {
+        if (CINR == 4 * CG || 4 * cg + j < CINR) {
+          const float4 v = __ldg(reinterpret_cast<const float4*>(src + (size_t)j * plane));
+          c[j] = make_float4(umma::to_tf32(v.x), umma::to_tf32(v.y), umma::to_tf32(v.z), umma::to_tf32(v.w));
+        } else {
+          c[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+      }
+      float4* dst = As + (size_t)(cg * 3 + r) * kTcXW + 1 + 4 * k4;
+      dst[0] = make_float4(c[0].x, c[1].x, c[2].x, c[3].x);
+      dst[1] = make_float4(c[0].y, c[1].y, c[2].y, c[3].y);
+      dst[2] = make_float4(c[0].z, c[1].z, c[2].z, c[3].z);
+      dst[3] = make_float4(c[0].w, c[1].w, c[2].w, c[3].w);
     }
     // the two halo pixels of every row (periodic wrap in x)
-    for (int q = tid; q < kTcCG * (kTcRows + 2) * 2; q += 128) {
-      const int side = q & 1, rr = q >> 1, r = rr % (kTcRows + 2), cg = rr / (kTcRows + 2);
+    for (int q = tid; q < CG * 3 * 2; q += 128) {
+      const int side = q & 1, rr = q >> 1, r = rr % 3, cg = rr / 3;
       const int px = side ? kTcXW - 1 : 0;
-      const float* src =
-          inb + (size_t)(4 * cg) * plane + (size_t)wrap(y0 + r - 1, H) * W + wrap(x0 + px - 1, W);
-      As[(size_t)(cg * (kTcRows + 2) + r) * kTcXW + px] =
-          make_float4(umma::to_tf32(__ldg(src)), umma::to_tf32(__ldg(src + plane)),
-                      umma::to_tf32(__ldg(src + 2 * plane)), umma::to_tf32(__ldg(src + 3 * plane)));
+      const float* src = inb + (size_t)(4 * cg) * plane + (size_t)wrap(y0 + r - 1, H) * W + wrap(x0 + px - 1, W);
+      As[(size_t)(cg * 3 + r) * kTcXW + px] =
+          make_float4(chan(src, 4 * cg, 0), chan(src, 4 * cg, 1), chan(src, 4 * cg, 2), chan(src, 4 * cg, 3));
     }
     fence_proxy_async_smem();  // the operands are read by the tensor cores (async proxy)
     umma::fence_before_sync();
@@ -182,23 +202,21 @@ __global__ void __launch_bounds__(128, 1)
     umma::fence_after_sync();
     const unsigned tmem = *slot;
     if (tid == 0) {
-      bool wok = it > 0 || mbar_wait_bounded(&bars[0], 0, wait_ns);
+      const bool wok = it > 0 || mbar_wait_bounded(&bars[0], 0, wait_ns);
       if (wok) {
-        constexpr uint32_t idesc = umma::instr_desc(umma::kFmtTF32, kTcPix, kCnnHid);
+        constexpr uint32_t idesc = umma::instr_desc(umma::kFmtTF32, kTcPix, NN);
         const unsigned a0 = smem_u32(As), b0 = smem_u32(Bs);
 #pragma unroll 1
-        for (int r = 0; r < kTcRows; r++)
-#pragma unroll 1
-          for (int tap = 0; tap < 9; tap++) {
-            const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        for (int tap = 0; tap < 9; tap++) {
+          const int dy = tap / 3 - 1, dx = tap % 3 - 1;
 #pragma unroll
-            for (int s = 0; s < kTcCG / 2; s++) {  // channel groups 2s, 2s+1: K = 8
-              const unsigned aoff = (unsigned)((2 * s * kTcAPlane + (r + 1 + dy) * kTcXW + 1 + dx) * 16);
-              const unsigned boff = (unsigned)((tap * kTcCG + 2 * s) * kCnnHid * 16);
-              umma::mma_tf32(tmem + (unsigned)(r * kCnnHid), umma::smem_desc(a0 + aoff, kTcAPlane * 16, 128),
-                             umma::smem_desc(b0 + boff, kCnnHid * 16, 128), idesc, tap > 0 || s > 0);
-            }
+          for (int s = 0; s < CG / 2; s++) {  // channel groups 2s, 2s+1: K = 8
+            const unsigned aoff = (unsigned)((2 * s * kTcAPlane + (1 + dy) * kTcXW + 1 + dx) * 16);
+            const unsigned boff = (unsigned)((tap * CG + 2 * s) * NN * 16);
+            umma::mma_tf32(tmem, umma::smem_desc(a0 + aoff, kTcAPlane * 16, 128),
+                           umma::smem_desc(b0 + boff, NN * 16, 128), idesc, tap > 0 || s > 0);
           }
+        }
         umma::commit(&bars[1]);
       } else {
         atomicExch(status, TARA_ETIMEOUT);
@@ -210,23 +228,20 @@ __global__ void __launch_bounds__(128, 1)
     if (ok) ok = __syncthreads_and(mbar_wait_bounded(&bars[1], it & 1, wait_ns));
     umma::fence_after_sync();
     if (ok) {
-#pragma unroll 1
-      for (int r = 0; r < kTcRows; r++) {
-        float acc[kCnnHid];
-        umma::ld_32x32b_x32(tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(r * kCnnHid), acc);
-        const size_t po = (size_t)(y0 + r) * W + x0 + 32 * warp + lane;
+      float acc[32];  // columns NN..31 are not written by the MMAs and are not used
+      umma::ld_32x32b_x32(tmem + ((unsigned)(32 * warp) << 16), acc);
+      const size_t po = (size_t)y0 * W + x0 + 32 * warp + lane;
 #pragma unroll
-        for (int co = 0; co < kCnnHid; co++) {
-          const float v = acc[co] + (bias ? __ldg(bias + co) : 0.0f);
-          const size_t idx = ((size_t)b * kCnnHid + co) * plane + po;
-          if constexpr (EPI == EPI_GELU) {
-            z[idx] = v;
-            out[idx] = gelu(v);
-          } else if constexpr (EPI == EPI_LINEAR) {
-            out[idx] = v;
-          } else {
-            out[idx] = v * gelu_d(__ldg(zprev + idx));
-          }
+      for (int co = 0; co < COUT; co++) {
+        const float v = acc[co] + (bias ? __ldg(bias + co) : 0.0f);
+        const size_t idx = ((size_t)b * COUT + co) * plane + po;
+        if constexpr (EPI == EPI_GELU) {
+          z[idx] = v;
+          out[idx] = gelu(v);
+        } else if constexpr (EPI == EPI_LINEAR) {
+          out[idx] = v;
+        } else {
+          out[idx] = v * gelu_d(__ldg(zprev + idx));
         }
       }
     } else if (slot[1]) {
@@ -247,16 +262,19 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 0) umma::tmem_dealloc(*slot, kTcCols);
 }
 
-// master W[cout][cin][3][3] of a 32 -> 32 layer -> tensor-core B operands:
-// forward [tap][cin/4][cout][cin%4] and the input-gradient conv's
-// [mirrored tap][cout/4][cin][cout%4], BF16-rounded values as FP32
-__global__ void k_pack_weights_tc(const float* __restrict__ m, float* __restrict__ wf, float* __restrict__ wb) {
-  constexpr int C = kCnnHid, nw = C * C * 9;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x) {
-    const int co = i / (C * 9), ci = (i / 9) % C, tap = i % 9;
-    const float v = __bfloat162float(__float2bfloat16_rn(m[i]));
-    wf[((tap * kTcCG + ci / 4) * C + co) * 4 + ci % 4] = v;
-    wb[(((8 - tap) * kTcCG + co / 4) * C + ci) * 4 + co % 4] = v;
+// Tensor-core B operand of a layer W[cout][cin][3][3] (BF16-rounded values
+// as FP32), padded to cg channel groups of four and nn columns:
+//   forward:        [tap][ci/4][co][ci%4]          (inputs ci, outputs co)
+//   input gradient: [8 - tap][co/4][ci][co%4]      (inputs co, outputs ci)
+// Every entry of the padded shape is written (zero outside the layer).
+__global__ void k_pack_weights_tc(const float* __restrict__ m, int cin, int cout, int cg, int nn, int grad,
+                                  float* __restrict__ dst) {
+  const int n = 9 * cg * nn * 4;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i % 4, col = (i / 4) % nn, g = (i / (4 * nn)) % cg, t = i / (4 * nn * cg);
+    const int k = 4 * g + c;  // input channel of the convolution
+    const int ci = grad ? col : k, co = grad ? k : col, tap = grad ? 8 - t : t;
+    dst[i] = (ci < cin && co < cout) ? __bfloat162float(__float2bfloat16_rn(m[(co * cin + ci) * 9 + tap])) : 0.0f;
   }
 }
 
@@ -406,19 +424,27 @@ void launch_conv(const float* in, const __nv_bfloat16* w, const float* bias, flo
   }
   launch_conv_split<CIN, COUT, COUT, EPI>(in, w, bias, z, out, zprev, B, H, W, st);
 }
-template <int EPI>
+// Padded tensor-core shape of a convolution with cin inputs and cout
+// outputs: channel groups of four (an even number) and accumulator columns.
+inline int tc_groups(int cin) { return ((cin + 3) / 4 + 1) / 2 * 2; }
+inline int tc_cols(int cout) { return cout <= 16 ? 16 : 32; }
+
+template <int CG, int NN, int COUT, int CINR, int EPI>
 void launch_conv_tc(const float* in, const float* wtc, const float* bias, float* z, float* out, const float* zprev,
                     int B, int H, int W, int* status, unsigned long long wait_ns, cudaStream_t st) {
-  auto kern = k_conv_tc<EPI>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
-  // persistent: at most as many CTAs as fit, each loading the weights once
-  int per_sm = 1, dev = 0, sms = 148;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, kTcSmem);
+  using G = TcGeom<CG, NN>;
+  auto kern = k_conv_tc<CG, NN, COUT, CINR, EPI>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+  // persistent: at most as many CTAs as fit (by shared memory; the kernel's
+  // 128 threads leave registers for two), each loading the weights once
+  int dev = 0, sms = 148, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int ntiles = (W / kTcPix) * (H / kTcRows) * B;
-  const int grid = std::min(ntiles, std::max(per_sm, 1) * sms);
-  kern<<<grid, 128, kTcSmem, st>>>(in, wtc, bias, z, out, zprev, B, H, W, status, wait_ns);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  const int per_sm = std::max(1, std::min(2, optin / (int)(G::SMEM + 1024)));
+  const int ntiles = (W / kTcPix) * H * B;
+  const int grid = std::min(ntiles, per_sm * sms);
+  kern<<<grid, 128, G::SMEM, st>>>(in, wtc, bias, z, out, zprev, B, H, W, status, wait_ns);
 }
 template <int CIN, int COUT>
 void launch_dw(const float* in, const float* dz, float* part, float* g, int B, int H, int W, cudaStream_t st) {
@@ -434,10 +460,7 @@ void launch_dw(const float* in, const float* dz, float* part, float* g, int B, i
 
 int cnn_num_params() { return layer_offset(kCnnLayers); }
 
-bool Cnn::tc_layer(int l) const {
-  const CnnLayerDims d = cnn_layer(l);
-  return tensor_cores && d.cin == kCnnHid && d.cout == kCnnHid && W % kTcPix == 0 && H % kTcRows == 0;
-}
+bool Cnn::tc_layer(int) const { return tensor_cores && W % kTcPix == 0; }
 
 int Cnn::alloc(int H_, int W_, int Bmax_) {
   if (H_ % kTile || W_ % kTile || H_ < kTile || W_ < kTile || Bmax_ < 1) {
@@ -455,8 +478,8 @@ int Cnn::alloc(int H_, int W_, int Bmax_) {
     if (ok && d.gelu) ok = am((void**)&z[l], (size_t)Bmax * d.cout * plane * 4);
     if (ok) ok = am((void**)&a[l], (size_t)Bmax * d.cout * plane * 4);
     bias[l] = biasbuf + layer_offset(l) + d.cout * d.cin * 9;
-    if (ok && d.cin == kCnnHid && d.cout == kCnnHid)
-      ok = am((void**)&wtcf[l], kTcBBytes) && am((void**)&wtcb[l], kTcBBytes);
+    if (ok) ok = am((void**)&wtcf[l], (size_t)9 * tc_groups(d.cin) * tc_cols(d.cout) * 16);
+    if (ok && l > 0) ok = am((void**)&wtcb[l], (size_t)9 * tc_groups(d.cout) * tc_cols(d.cin) * 16);
   }
   if (ok) ok = am((void**)&status, sizeof(int));
   if (ok) ok = cudaMemset(status, 0, sizeof(int)) == cudaSuccess;
@@ -491,7 +514,12 @@ int Cnn::refresh(cudaStream_t st) {
     const CnnLayerDims d = cnn_layer(l);
     k_pack_weights<<<64, 256, 0, st>>>(master + layer_offset(l), d.cin, d.cout, wfwd[l], wbwd[l],
                                        biasbuf + layer_offset(l));
-    if (wtcf[l]) k_pack_weights_tc<<<36, 256, 0, st>>>(master + layer_offset(l), wtcf[l], wtcb[l]);
+    if (wtcf[l])
+      k_pack_weights_tc<<<36, 256, 0, st>>>(master + layer_offset(l), d.cin, d.cout, tc_groups(d.cin),
+                                            tc_cols(d.cout), 0, wtcf[l]);
+    if (wtcb[l])
+      k_pack_weights_tc<<<36, 256, 0, st>>>(master + layer_offset(l), d.cin, d.cout, tc_groups(d.cout),
+                                            tc_cols(d.cin), 1, wtcb[l]);
   }
   TARA_CUDA_TRY(cudaGetLastError());
   return TARA_OK;
@@ -499,31 +527,46 @@ int Cnn::refresh(cudaStream_t st) {
 
 int Cnn::forward(const float* in, int B, bool, cudaStream_t st) {
   if (B < 1 || B > Bmax) { set_error("batch larger than the CNN buffers"); return TARA_EINVAL; }
-  launch_conv<kCnnIn, kCnnHid, EPI_GELU>(in, wfwd[0], bias[0], z[0], a[0], nullptr, B, H, W, st);
-  for (int l = 1; l <= 2; l++) {
-    if (tc_layer(l))
-      launch_conv_tc<EPI_GELU>(a[l - 1], wtcf[l], bias[l], z[l], a[l], nullptr, B, H, W, status, wait_ns, st);
-    else
+  if (tc_layer(0)) {
+    // all four layers on the tensor cores (padded shapes: 5 inputs in two
+    // channel groups, 4 outputs in an N = 16 tile)
+    launch_conv_tc<2, 32, kCnnHid, kCnnIn, EPI_GELU>(in, wtcf[0], bias[0], z[0], a[0], nullptr, B, H, W, status,
+                                                      wait_ns, st);
+    for (int l = 1; l <= 2; l++)
+      launch_conv_tc<8, 32, kCnnHid, kCnnHid, EPI_GELU>(a[l - 1], wtcf[l], bias[l], z[l], a[l], nullptr, B, H, W,
+                                                         status, wait_ns, st);
+    launch_conv_tc<8, 16, kCnnOut, kCnnHid, EPI_LINEAR>(a[2], wtcf[3], bias[3], nullptr, a[3], nullptr, B, H, W,
+                                                         status, wait_ns, st);
+  } else {
+    launch_conv<kCnnIn, kCnnHid, EPI_GELU>(in, wfwd[0], bias[0], z[0], a[0], nullptr, B, H, W, st);
+    for (int l = 1; l <= 2; l++)
       launch_conv<kCnnHid, kCnnHid, EPI_GELU>(a[l - 1], wfwd[l], bias[l], z[l], a[l], nullptr, B, H, W, st);
+    launch_conv<kCnnHid, kCnnOut, EPI_LINEAR>(a[2], wfwd[3], bias[3], nullptr, a[3], nullptr, B, H, W, st);
   }
-  launch_conv<kCnnHid, kCnnOut, EPI_LINEAR>(a[2], wfwd[3], bias[3], nullptr, a[3], nullptr, B, H, W, st);
   TARA_CUDA_TRY(cudaGetLastError());
   return TARA_OK;
 }
 
 int Cnn::backward(const float* in, const float* dout, int B, cudaStream_t st) {
   if (B < 1 || B > Bmax) { set_error("batch larger than the CNN buffers"); return TARA_EINVAL; }
+  const bool tc = tc_layer(0);
   // layer 3 (linear): dout is the gradient of its pre-activation
   launch_dw<kCnnHid, kCnnOut>(a[2], dout, part, grad + layer_offset(3), B, H, W, st);
-  launch_conv<kCnnOut, kCnnHid, EPI_GELUGRAD>(dout, wbwd[3], nullptr, nullptr, dz[0], z[2], B, H, W, st);
+  if (tc)
+    launch_conv_tc<2, 32, kCnnHid, kCnnOut, EPI_GELUGRAD>(dout, wtcb[3], nullptr, nullptr, dz[0], z[2], B, H, W,
+                                                           status, wait_ns, st);
+  else
+    launch_conv<kCnnOut, kCnnHid, EPI_GELUGRAD>(dout, wbwd[3], nullptr, nullptr, dz[0], z[2], B, H, W, st);
   launch_dw<kCnnHid, kCnnHid>(a[1], dz[0], part, grad + layer_offset(2), B, H, W, st);
-  if (tc_layer(2))
-    launch_conv_tc<EPI_GELUGRAD>(dz[0], wtcb[2], nullptr, nullptr, dz[1], z[1], B, H, W, status, wait_ns, st);
+  if (tc)
+    launch_conv_tc<8, 32, kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[0], wtcb[2], nullptr, nullptr, dz[1], z[1], B, H, W,
+                                                           status, wait_ns, st);
   else
     launch_conv<kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[0], wbwd[2], nullptr, nullptr, dz[1], z[1], B, H, W, st);
   launch_dw<kCnnHid, kCnnHid>(a[0], dz[1], part, grad + layer_offset(1), B, H, W, st);
-  if (tc_layer(1))
-    launch_conv_tc<EPI_GELUGRAD>(dz[1], wtcb[1], nullptr, nullptr, dz[0], z[0], B, H, W, status, wait_ns, st);
+  if (tc)
+    launch_conv_tc<8, 32, kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[1], wtcb[1], nullptr, nullptr, dz[0], z[0], B, H, W,
+                                                           status, wait_ns, st);
   else
     launch_conv<kCnnHid, kCnnHid, EPI_GELUGRAD>(dz[1], wbwd[1], nullptr, nullptr, dz[0], z[0], B, H, W, st);
   launch_dw<kCnnIn, kCnnHid>(in, dz[0], part, grad + layer_offset(0), B, H, W, st);

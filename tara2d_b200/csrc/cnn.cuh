@@ -1,10 +1,10 @@
 // The closure CNN: 4 periodic 3x3 convolutions, channels
 // 5 -> 32 -> 32 -> 32 -> 4, GELU after the first three.  Weights are kept as
 // FP32 masters (the optimiser's copy) and used rounded to BF16; accumulation
-// is FP32.  The 32 -> 32 convolutions (forward and input gradient) run on
-// the tensor cores (tcgen05 MMAs, TF32 activations) unless tensor_cores is
-// 0; the others, and the weight gradients, on CUDA cores with FP32
-// activations.  Hand-written forward, input-gradient and weight-gradient
+// is FP32.  Every convolution (forward and input gradient) runs on the
+// tensor cores (tcgen05 MMAs, TF32 activations) when the plane width is a
+// multiple of 128, unless tensor_cores is 0; then, and for the weight
+// gradients, CUDA cores with FP32 activations.  Hand-written forward, input-gradient and weight-gradient
 // kernels; Adam on the masters.
 //
 // Tensors are [B][C][H][W] FP32 (H, W multiples of 16).  Flat parameter
@@ -42,15 +42,15 @@ struct Cnn {
   float* dz[2] = {};                      // ping-pong gradients w.r.t. pre-activations
   float* part = nullptr;                  // per-CTA weight-gradient partials
   size_t part_elems = 0;
-  // tensor cores (tcgen05, TF32 activations) for the 32 -> 32 convolutions;
-  // 0: every convolution on CUDA cores with FP32 activations (the reference
-  // of the tensor-core path)
+  // tensor cores (tcgen05, TF32 activations) for the convolutions; 0: every
+  // convolution on CUDA cores with FP32 activations (the reference of the
+  // tensor-core path)
   int tensor_cores = 1;
-  float* wtcf[kCnnLayers] = {};           // tensor-core B operands, forward (32 -> 32 layers)
-  float* wtcb[kCnnLayers] = {};           // and of their input-gradient convolutions
+  float* wtcf[kCnnLayers] = {};           // tensor-core B operands of the forward convolutions
+  float* wtcb[kCnnLayers] = {};           // and of the input-gradient convolutions (layers 1..3)
   int* status = nullptr;                  // device word: TARA_ETIMEOUT when a bounded wait ran out
   unsigned long long wait_ns = 1000000000ull;
-  bool tc_layer(int l) const;             // layer l's convolutions run on the tensor cores
+  bool tc_layer(int l) const;             // the convolutions run on the tensor cores
   double* lossacc = nullptr;
   long long adam_t = 0;
   int alloc(int H, int W, int Bmax);

@@ -1,15 +1,16 @@
 """The closure CNN's tensor-core convolutions (tcgen05, kind::tf32) against
 PyTorch references of the same network.
 
-On planes whose width is a multiple of 128 the two 32 -> 32 convolutions run
-as tcgen05 MMAs whose activations enter rounded to TF32 (round to nearest,
-ties away from zero: what cvt.rna.tf32.f32 does) while the BF16 weights are
-exact in TF32 and accumulation is FP32.  Tolerances:
-  * forward against a PyTorch FP32 network whose inputs to those two
-    convolutions are rounded to TF32 the same way: relative L2 <= 1e-4 (the
+On planes whose width is a multiple of 128 every convolution (the four
+layers forward and the input gradients) runs as tcgen05 MMAs whose
+activations enter rounded to TF32 (round to nearest, ties away from zero:
+what cvt.rna.tf32.f32 does) while the BF16 weights are exact in TF32 and
+accumulation is FP32.  Tolerances:
+  * forward against a PyTorch FP32 network whose inputs to every
+    convolution are rounded to TF32 the same way: relative L2 <= 1e-4 (the
     accumulation order differs, and a value that lands within an FP32 ulp of
-    a TF32 rounding boundary before the second tensor-core layer may round to
-    the other neighbour, one TF32 ulp (2^-11) away);
+    a TF32 rounding boundary before a later layer may round to the other
+    neighbour, one TF32 ulp (2^-11) away);
   * forward against plain FP32 PyTorch and against the CUDA-core path of the
     same closure: <= 3e-3 (the TF32 rounding of the activations);
   * parameter gradients against plain FP32 PyTorch: <= 1e-2 per layer (the
@@ -33,12 +34,12 @@ def _tf32(t):
     return (r | (b & -0x80000000)).view(torch.float32)
 
 
-def _net(w, x, tf32_hidden):
+def _net(w, x, tf32_inputs):
     h = torch.tensor(x)
-    for l, ((W, b), (ci, co, act)) in enumerate(zip(_unflatten(w), _layers())):
+    for (W, b), (_, _, act) in zip(_unflatten(w), _layers()):
         Wq = W.to(torch.bfloat16).to(torch.float32)
         bq = b.to(torch.bfloat16).to(torch.float32)
-        if tf32_hidden and ci == 32 and co == 32:
+        if tf32_inputs:
             h = _tf32(h)
         h = F.conv2d(F.pad(h, (1, 1, 1, 1), mode="circular"), Wq, bq)
         if act:
