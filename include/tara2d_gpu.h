@@ -294,10 +294,11 @@ int tara_filter_state(tara_session* fine, tara_session* coarse);
  * mu, eta, CS, dt with A = 0 and fix_curlB = 0; members of one grid size
  * share Lx, Ly, pi), advanced together: each step is three persistent
  * launches over every hydro member (column inverse, row pass, column forward
- * with the AB2/Euler update) and four over every MHD member (first row pass,
- * d(uy)/dy, second row pass, column forward with the update and the y-inverse
- * of the new state; a column inverse first where the state was just set),
- * replayed from a CUDA graph.  Each member is bit-identical to a session run
+ * with the AB2/Euler update) and one over every MHD member (a cooperative
+ * launch whose phases, separated by grid-wide barriers, are the first row
+ * pass, d(uy)/dy, the second row pass and the column forward with the update
+ * and the y-inverse of the new state; a column inverse first where the state
+ * was just set), replayed from a CUDA graph.  Each member is bit-identical to a session run
  * of it.  State arrays are complex(8) (Nh,Ny) host arrays as for sessions,
  * tara_ens_num_fields(e, m) of them (3 hydro, 6 MHD); AB2 history starts at
  * zero.  FP32 or FP64 fields; diagnostics sum in FP64. */

@@ -12,9 +12,12 @@
 //   k_ens_row      items (member, block of rows): the hydro row pass
 //   k_ens_col_fwd  items (member, column tile, field): y-forward, mask, AB2
 //
-// MHD members, four launches (a fifth, the column inverse, only where the
-// half-real fields do not hold the y-inverse of the state yet: the column
-// forward pass writes it for the next step, as in a single-grid session):
+// MHD members, one persistent cooperative launch per step (k_ens_com_step)
+// that runs these phases one after another, separated by grid-wide barriers
+// with bounded waits (where the device has no cooperative launches, one
+// launch per phase; the column inverse only where the half-real fields do
+// not hold the y-inverse of the state yet: the column forward pass writes it
+// for the next step, as in a single-grid session):
 //
 //   k_ens_com_inv   items (member, column tile, job): y-inverse of 6 fields
 //   k_ens_com_row1  items (member, block of rows): c2r, fluxes, 8 r2c
@@ -26,7 +29,7 @@
 // Each kernel runs a grid of (CTAs per SM) x (SMs) CTAs that walk a
 // size-sorted item list (largest grids first), so members of every size share
 // every launch; the phase boundaries are the only synchronisation.  A step is
-// the same launches for any mix of members (three for the hydro members, four
+// the same launches for any mix of members (three for the hydro members, one
 // for the MHD ones), so step pairs are captured once into a CUDA graph and
 // replayed.  Per-member arithmetic is the same
 // device code as a single-grid session (col_inv_tile, row_coh_rows,
@@ -198,9 +201,10 @@ template <class T> constexpr int ens_com_minb() { return sizeof(T) == 4 ? 4 : 2;
   case 384: FN(384); break;    \
   case 512: FN(512); break;
 
+// The five MHD phases as loops of the calling CTA over its share of a phase's
+// items (item it of CTA b: it = b, b + gridDim.x, ...).
 template <class T>
-__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
-    k_ens_com_inv(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems, int parity) {
+__device__ __forceinline__ void ens_com_inv(const EnsComMember<T>* mem, const int4* items, int nitems, int parity) {
   extern __shared__ __align__(16) unsigned char smraw[];
   Cx<T>* sm = reinterpret_cast<Cx<T>*>(smraw);
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -216,8 +220,7 @@ __global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
   }
 }
 template <class T>
-__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
-    k_ens_com_row1(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+__device__ __forceinline__ void ens_com_row1(const EnsComMember<T>* mem, const int4* items, int nitems) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int4 w = items[it];
     const EnsComMember<T>& m = mem[w.x];
@@ -229,8 +232,7 @@ __global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
   }
 }
 template <class T>
-__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
-    k_ens_com_rt(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+__device__ __forceinline__ void ens_com_rt(const EnsComMember<T>* mem, const int4* items, int nitems) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int4 w = items[it];
     const EnsComMember<T>& m = mem[w.x];
@@ -241,8 +243,7 @@ __global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
   }
 }
 template <class T>
-__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
-    k_ens_com_row2(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+__device__ __forceinline__ void ens_com_row2(const EnsComMember<T>* mem, const int4* items, int nitems) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int4 w = items[it];
     const EnsComMember<T>& m = mem[w.x];
@@ -253,8 +254,7 @@ __global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
   }
 }
 template <class T>
-__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
-    k_ens_com_fwd(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems, int parity) {
+__device__ __forceinline__ void ens_com_fwd(const EnsComMember<T>* mem, const int4* items, int nitems, int parity) {
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int4 w = items[it];
     const EnsComMember<T>& m = mem[w.x];
@@ -264,6 +264,99 @@ __global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
 #undef TARA_EC_FWD
     __syncthreads();
   }
+}
+
+// One launch per phase (the fallback where cooperative launches are not
+// available).
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_inv(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems, int parity) {
+  ens_com_inv<T>(mem, items, nitems, parity);
+}
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_row1(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+  ens_com_row1<T>(mem, items, nitems);
+}
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_rt(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+  ens_com_rt<T>(mem, items, nitems);
+}
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_row2(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems) {
+  ens_com_row2<T>(mem, items, nitems);
+}
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_fwd(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ items, int nitems, int parity) {
+  ens_com_fwd<T>(mem, items, nitems, parity);
+}
+
+// Grid-wide barrier of a cooperative launch (every CTA resident): one
+// arrival counter and a generation word in global memory, zero when the
+// ensemble is made and back to a zero count after every barrier.  Thread 0
+// of each CTA arrives; the last to arrive resets the count and advances the
+// generation, the others wait for the generation to change for at most
+// limit_ns of %globaltimer.  false (on every thread) if the wait ran out.
+struct EnsGridBar {
+  unsigned count;
+  unsigned gen;
+};
+__device__ __forceinline__ bool ens_grid_sync(EnsGridBar* bar, unsigned long long limit_ns) {
+  __syncthreads();
+  bool ok = true;
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = &bar->gen;
+    const unsigned g = *gen;
+    __threadfence();  // this CTA's writes before its arrival
+    if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      while (*gen == g) {
+        if (global_ns() - t0 > limit_ns) {
+          ok = false;
+          break;
+        }
+      }
+    }
+    __threadfence();  // the other CTAs' writes after the barrier
+  }
+  return __syncthreads_and(ok);
+}
+
+// A whole MHD ensemble step in one persistent, cooperative launch: the
+// phases (column inverse where `first`, row pass 1, d(uy)/dy, row pass 2,
+// column forward + update) one after another, separated by grid barriers.
+// A barrier that runs out records TARA_ETIMEOUT in *status and ends the
+// step (the members' state is then not advanced consistently; the host
+// reports the error).
+template <class T>
+__global__ void __launch_bounds__(kEnsComThreads, ens_com_minb<T>())
+    k_ens_com_step(const EnsComMember<T>* __restrict__ mem, const int4* __restrict__ inv, int ninv,
+                   const int4* __restrict__ row1, int nrow1, const int4* __restrict__ rt, int nrt,
+                   const int4* __restrict__ row2, int nrow2, const int4* __restrict__ fwd, int nfwd, int parity,
+                   int first, EnsGridBar* bar, int* status, unsigned long long wait_ns) {
+  auto sync = [&]() {
+    if (ens_grid_sync(bar, wait_ns)) return true;
+    if (threadIdx.x == 0) atomicExch(status, TARA_ETIMEOUT);
+    return false;
+  };
+  if (first) {
+    ens_com_inv<T>(mem, inv, ninv, parity);
+    if (!sync()) return;
+  }
+  ens_com_row1<T>(mem, row1, nrow1);
+  if (!sync()) return;
+  ens_com_rt<T>(mem, rt, nrt);
+  if (!sync()) return;
+  ens_com_row2<T>(mem, row2, nrow2);
+  if (!sync()) return;
+  ens_com_fwd<T>(mem, fwd, nfwd, parity);
 }
 
 // dynamic shared memory of each MHD phase kernel: the largest over the sizes
@@ -405,6 +498,9 @@ struct EnsembleT : tara_ensemble {
   // the MHD members' half-real fields hold the y-inverse of their current
   // state (written by the previous column forward pass)
   bool com_h_valid = false;
+  // MHD step as one cooperative launch (else one launch per phase)
+  bool com_coop = false;
+  EnsGridBar* dbar = nullptr;
   int tuning[6] = {16, 16, 16, 0, 0, 0};  // P col_inv, P row, P col_fwd, CTAs/SM of each (0 = most that fit)
   int parity = 0;
   int built_mode = -1;
@@ -425,6 +521,7 @@ struct EnsembleT : tara_ensemble {
       if (p) cudaFree(p);
     if (dmem) cudaFree(dmem);
     if (dcom) cudaFree(dcom);
+    if (dbar) cudaFree(dbar);
     if (arena) cudaFree(arena);
     if (stage) cudaFree(stage);
     if (drec) cudaFree(drec);
@@ -483,7 +580,17 @@ struct EnsembleT : tara_ensemble {
     TARA_CUDA_TRY(cudaMalloc(&stage, maxh * sizeof(Cx<double>)));
     TARA_CUDA_TRY(cudaMalloc(&drec, (kDiagOut + 1024) * sizeof(double)));
     if (nhyd) TARA_CUDA_TRY(cudaMalloc(&dmem, (size_t)nhyd * sizeof(EnsMember<T>)));
-    if (ncom) TARA_CUDA_TRY(cudaMalloc(&dcom, (size_t)ncom * sizeof(EnsComMember<T>)));
+    if (ncom) {
+      TARA_CUDA_TRY(cudaMalloc(&dcom, (size_t)ncom * sizeof(EnsComMember<T>)));
+      int dev = 0, coop = 0;
+      TARA_CUDA_TRY(cudaGetDevice(&dev));
+      TARA_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+      if (coop) {
+        TARA_CUDA_TRY(cudaMalloc(&dbar, sizeof(EnsGridBar)));
+        TARA_CUDA_TRY(cudaMemsetAsync(dbar, 0, sizeof(EnsGridBar), st));
+        com_coop = true;
+      }
+    }
     build_members();
     TARA_TRY(upload_members());
     TARA_TRY(build_items());
@@ -741,13 +848,41 @@ struct EnsembleT : tara_ensemble {
     }
     return TARA_OK;
   }
+  // the MHD phases of one step in one cooperative launch: as many CTAs as are
+  // resident at once (the grid barriers need all of them)
+  int launch_com_step(int par, bool first) {
+    const size_t smem =
+        std::max(ens_com_col_smem<T>(), std::max(ens_com_row_smem<T>(1), ens_com_row_smem<T>(2)));
+    int grid = 0;
+    TARA_TRY(grid_of(k_ens_com_step<T>, kEnsComThreads, smem, 0, grid));
+    const Tables<T>& tb = grids.begin()->second->tb;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kEnsComThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TARA_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_ens_com_step<T>, (const EnsComMember<T>*)dcom, (const int4*)citems[0],
+                                     ncitems[0], (const int4*)citems[1], ncitems[1], (const int4*)citems[2],
+                                     ncitems[2], (const int4*)citems[3], ncitems[3], (const int4*)citems[4],
+                                     ncitems[4], par, first ? 1 : 0, dbar, tb.status, tb.wait_ns));
+    return TARA_OK;
+  }
   int launch_steps(int n_) {
     for (int s = 0; s < n_; s++) {
       TARA_TRY(launch_inv(parity));
       TARA_TRY(launch_row());
       TARA_TRY(launch_fwd(parity));
       if (ncom) {
-        for (int ph = com_h_valid ? 1 : 0; ph < 5; ph++) TARA_TRY(launch_com(ph, parity));
+        if (com_coop) {
+          TARA_TRY(launch_com_step(parity, !com_h_valid));
+        } else {
+          for (int ph = com_h_valid ? 1 : 0; ph < 5; ph++) TARA_TRY(launch_com(ph, parity));
+        }
         com_h_valid = true;  // the column forward pass wrote the y-inverse of the new state
       }
       TARA_CUDA_TRY(cudaGetLastError());
