@@ -262,6 +262,11 @@ int tara_closure_close(tara_closure* c);
 int tara_closure_num_params(void);
 int tara_closure_count(const tara_closure* c);
 int tara_closure_add_pair(tara_closure* c, tara_session* fine);
+/* The same from the current state of member `member` of an ensemble: an FP64
+ * MHD member whose grid the closure grid divides (so a batch of DNS runs
+ * advanced together as one ensemble produces the training data). */
+struct tara_ensemble;
+int tara_closure_add_pair_member(tara_closure* c, struct tara_ensemble* e, int member);
 int tara_closure_get_pair(tara_closure* c, int idx, float* in5, float* out4);
 int tara_closure_get_norm(const tara_closure* c, float* norm18); /* mean_in[5] std_in[5] mean_out[4] std_out[4] */
 int tara_closure_set_norm(tara_closure* c, const float* norm18);

@@ -119,6 +119,7 @@ def lib():
         L.tara_closure_forward.argtypes = [P, P, I, P]
         L.tara_closure_backward.argtypes = [P, P, P, I, P]
         L.tara_closure_set_tensor_cores.argtypes = [P, I]
+        L.tara_closure_add_pair_member.argtypes = [P, P, I]
         L.tara_closure_status.argtypes = [P]
         L.tara_closure_time_cnn.argtypes = [P, I, I, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.tara_session_attach_closure.argtypes = [P, P]
@@ -577,6 +578,10 @@ class Closure:
 
     def add_pair(self, fine: "Session") -> None:
         check(lib().tara_closure_add_pair(self._h, fine._h), "tara_closure_add_pair")
+
+    def add_pair_member(self, ens: "Ensemble", member: int) -> None:
+        """A training pair from the current state of an FP64 MHD ensemble member."""
+        check(lib().tara_closure_add_pair_member(self._h, ens._h, member), "tara_closure_add_pair_member")
 
     def get_pair(self, idx: int):
         n = self.Nc

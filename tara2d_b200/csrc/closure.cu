@@ -204,15 +204,15 @@ int closure_terms(tara_closure* c, const Grid<double>& g, Cx<double>* const* in,
 
 namespace {
 
-int add_pair(tara_closure* c, tara_session* fine) {
-  if (fine->model != TARA_MODEL_COM || fine->precision != TARA_FP64 || fine->Nx != fine->Ny ||
-      fine->Nx % c->Nc != 0) {
-    set_error("training pairs come from an FP64 MHD session on a square grid that the closure grid divides");
+// One training pair from an FP64 MHD state on the fine grid fg (six
+// spectral fields, last written on stream src).
+int add_pair_from(tara_closure* c, const Grid<double>& fg, Cx<double>* const* fstate, cudaStream_t src) {
+  if (fg.Nx != fg.Ny || fg.Nx % c->Nc != 0) {
+    set_error("training pairs come from an FP64 MHD state on a square grid that the closure grid divides");
     return TARA_EINVAL;
   }
   if (c->count >= c->cap) { set_error("the closure's dataset is full"); return TARA_EINVAL; }
-  const int Nf = fine->Nx, Nc = c->Nc;
-  const Grid<double>& fg = *static_cast<const Grid<double>*>(fine->grid_ptr());
+  const int Nf = fg.Nx, Nc = c->Nc;
   if (c->Nf != Nf) {
     if (c->rf) cudaFree(c->rf);
     c->rf = nullptr;
@@ -223,7 +223,7 @@ int add_pair(tara_closure* c, tara_session* fine) {
     TARA_TRY(c->fs.alloc(fg, 4, c->st));
     TARA_TRY(c->fw.alloc(fg, 6, c->st));
   }
-  TARA_CUDA_TRY(cudaStreamSynchronize(fine->st));
+  TARA_CUDA_TRY(cudaStreamSynchronize(src));
   cudaStream_t st = c->st;
   const size_t nf = (size_t)Nf * Nf, nc = (size_t)Nc * Nc;
   // fine state in real space, its nonlinear fluxes, their spectra
@@ -231,7 +231,7 @@ int add_pair(tara_closure* c, tara_session* fine) {
   double* rf[10];
   Cx<double>* fw[6];
   for (int k = 0; k < 6; k++) {
-    state[k] = static_cast<Cx<double>*>(fine->state_ptr(k));
+    state[k] = fstate[k];
     fw[k] = c->fw[k];
   }
   for (int k = 0; k < 10; k++) rf[k] = c->rf + k * nf;
@@ -264,6 +264,15 @@ int add_pair(tara_closure* c, tara_session* fine) {
   TARA_CUDA_TRY(cudaStreamSynchronize(st));
   c->count++;
   return TARA_OK;
+}
+int add_pair(tara_closure* c, tara_session* fine) {
+  if (fine->model != TARA_MODEL_COM || fine->precision != TARA_FP64) {
+    set_error("training pairs come from an FP64 MHD session on a square grid that the closure grid divides");
+    return TARA_EINVAL;
+  }
+  Cx<double>* state[6];
+  for (int k = 0; k < 6; k++) state[k] = static_cast<Cx<double>*>(fine->state_ptr(k));
+  return add_pair_from(c, *static_cast<const Grid<double>*>(fine->grid_ptr()), state, fine->st);
 }
 
 // one pass over samples [first, first + count) in batches; train: shuffled,
@@ -364,6 +373,15 @@ int tara_closure_count(const tara_closure* c) { return c ? c->count : 0; }
 int tara_closure_add_pair(tara_closure* c, tara_session* fine) {
   if (!c || !fine) return TARA_EINVAL;
   return add_pair(c, fine);
+}
+// a training pair from the current state of FP64 MHD ensemble member m
+int tara_closure_add_pair_member(tara_closure* c, tara_ensemble* e, int member) {
+  if (!c || !e) return TARA_EINVAL;
+  const Grid<double>* g = nullptr;
+  Cx<double>* state[6];
+  cudaStream_t st = nullptr;
+  TARA_TRY(ens_member_state(e, member, &g, state, &st));
+  return add_pair_from(c, *g, state, st);
 }
 int tara_closure_get_pair(tara_closure* c, int idx, float* in5, float* out4) {
   if (!c || idx < 0 || idx >= c->count || !in5 || !out4) return TARA_EINVAL;

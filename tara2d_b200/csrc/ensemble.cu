@@ -54,6 +54,7 @@
 #include "coh_impl.cuh"
 #include "com_impl.cuh"
 #include "diag.cuh"
+#include "closure.h"
 
 using namespace tara;
 
@@ -469,6 +470,8 @@ struct tara_ensemble {
   virtual int num_shells(int m) = 0;
   virtual int num_fields(int m) const = 0;
   virtual int device_status() = 0;
+  // FP64 MHD member m: its grid and six state fields (else TARA_EINVAL)
+  virtual int member_state(int m, const void** grid, void** state6) = 0;
 };
 
 namespace {
@@ -536,6 +539,15 @@ struct EnsembleT : tara_ensemble {
 
   int nfields(int m) const { return model[m] == TARA_MODEL_COM ? 6 : 3; }
   int num_fields(int m) const override { return m >= 0 && m < n ? nfields(m) : 0; }
+  int member_state(int m, const void** grid, void** state6) override {
+    if (m < 0 || m >= n || model[m] != TARA_MODEL_COM || sizeof(T) != sizeof(double)) {
+      set_error("training pairs come from an FP64 MHD ensemble member");
+      return TARA_EINVAL;
+    }
+    *grid = grids[N[m]].get();
+    for (int q = 0; q < 6; q++) state6[q] = fptr(m, 0, q);
+    return TARA_OK;
+  }
   int init(const int* models, const int* Nin, const tara_params* p) override {
     N.assign(Nin, Nin + n);
     model.assign(models, models + n);
@@ -1103,6 +1115,19 @@ struct EnsembleT : tara_ensemble {
 };
 
 }  // namespace
+
+namespace tara {
+int ens_member_state(tara_ensemble* e, int m, const Grid<double>** g, Cx<double>** state6, cudaStream_t* st) {
+  const void* gp = nullptr;
+  void* sp[6];
+  const int r = e->member_state(m, &gp, sp);
+  if (r != TARA_OK) return r;
+  *g = static_cast<const Grid<double>*>(gp);
+  for (int q = 0; q < 6; q++) state6[q] = static_cast<Cx<double>*>(sp[q]);
+  *st = e->st;
+  return TARA_OK;
+}
+}  // namespace tara
 
 extern "C" {
 

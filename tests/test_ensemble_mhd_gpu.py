@@ -166,3 +166,32 @@ def test_mhd_ensemble_errors(tara):
         assert tara.lib().tara_ens_num_fields(e._h, 1) == 6
         with pytest.raises(tara.TaraError):
             e.set_state(1, I.coh_random_phase(128, 128, seed=1))  # 3 fields for an MHD member
+
+
+def test_closure_pairs_from_ensemble_members(tara):
+    """Training pairs of the learned closure taken from FP64 MHD ensemble
+    members (a batch of fine runs stepped together) are bit-identical to pairs
+    taken from sessions holding the same states."""
+    sizes, mus = [256, 128], [1e-3, 2e-3]
+    _, params, states = _com_members(tara, sizes, mus)
+    nsteps = 4
+    with tara.Ensemble(sizes, params, precision=tara.FP64, model=tara.MODEL_COM) as e, \
+            tara.Closure(64, 4) as c_ens, tara.Closure(64, 4) as c_ses:
+        for m, st in enumerate(states):
+            e.set_state(m, st)
+        e.step(tara.STEP_AB2, nsteps)
+        for m in range(2):
+            c_ens.add_pair_member(e, m)
+        for m, N in enumerate(sizes):
+            with tara.Session(tara.MODEL_COM, N, N, params[m], precision=tara.FP64) as s:
+                s.set_state(states[m])
+                s.step(tara.STEP_AB2, nsteps)
+                c_ses.add_pair(s)
+        assert c_ens.count == 2 and c_ses.count == 2
+        for m in range(2):
+            for a, b in zip(c_ens.get_pair(m), c_ses.get_pair(m)):
+                assert np.array_equal(a, b), m
+        with pytest.raises(tara.TaraError):  # hydro or FP32 members give no pairs
+            with tara.Ensemble([128], tara.Params.make(**com_kw()), precision=tara.FP32,
+                               model=tara.MODEL_COM) as e32:
+                c_ens.add_pair_member(e32, 0)
