@@ -239,7 +239,7 @@ template <int L, int B, int P_> struct BatchFFT {
 
   // element index (t, i) of input value r of butterfly q (thread tid) at stage s
   template <int s>
-  TARA_HD static void in_pos(int tid, int q, int r, int& t, int& i) {
+  TARA_HD static constexpr void in_pos(int tid, int q, int r, int& t, int& i) {
     constexpr int R = Pl::R[s];
     int b = tid + q * NT;
     t = b % B;
@@ -247,13 +247,36 @@ template <int L, int B, int P_> struct BatchFFT {
     i = j + r * (L / R);
   }
   template <int s>
-  TARA_HD static void out_pos(int tid, int q, int r, int& t, int& i) {
+  TARA_HD static constexpr void out_pos(int tid, int q, int r, int& t, int& i) {
     constexpr int R = Pl::R[s];
     constexpr int Ns = stage_ns<L, P_>(s);
     int b = tid + q * NT;
     t = b % B;
     int j = b / B;
     i = (j / Ns) * Ns * R + (j % Ns) + r * Ns;
+  }
+  // True when the exchange in front of stage s (s >= 1) is a swap between
+  // threads tid and tid ^ 16 of 32: one transform (B = 1) on 32 threads whose
+  // stage s is radix 2, and every input of stage s either already sits in its
+  // thread's slot 2q + hb or sits in the partner's slot 2q + hb (hb = bit 4
+  // of tid), checked against in_pos/out_pos for every thread and slot.  Holds
+  // for the 512-point transforms with 16 values per thread (stages 16, 16, 2).
+  template <int s>
+  TARA_HDC static constexpr bool halves_exchange() {
+    if (B != 1 || NT != 32 || Pl::R[s] != 2) return false;
+    constexpr int Rp = Pl::R[s - 1];
+    for (int tid = 0; tid < 32; tid++) {
+      const int hb = (tid >> 4) & 1;
+      for (int q = 0; q < P / 2; q++)
+        for (int r = 0; r < 2; r++) {
+          int t = 0, i = 0, ts = 0, is = 0;
+          in_pos<s>(tid, q, r, t, i);
+          const int src = r == hb ? tid : tid ^ 16, slot = 2 * q + hb;
+          out_pos<s - 1>(src, slot / Rp, slot % Rp, ts, is);
+          if (is != i) return false;
+        }
+    }
+    return true;
   }
   // twiddle + butterflies of stage s on v[P] (v[q*R + r] = input r of butterfly q).
   // tw[m] = e^{-2 pi i m / L} (forward table); DIR selects the conjugate.

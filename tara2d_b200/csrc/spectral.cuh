@@ -105,14 +105,32 @@ __device__ __forceinline__ void fft_load(const Cx<T>* sm, int tid, Cx<T>* v) {
       v[q * R + r] = sm[F::sidx(t, i)];
     }
 }
+// The exchange of BatchFFT::halves_exchange in registers: each thread keeps
+// slot 2q + hb and trades slot 2q + 1 - hb with lane tid ^ 16 (tid is the
+// lane: the transform's 32 threads are one whole warp).
+template <class F, class T> __device__ __forceinline__ void warp_halves_swap(int tid, Cx<T>* v) {
+  const bool hi = tid & 16;
+#pragma unroll
+  for (int q = 0; q < F::P / 2; q++) {
+    Cx<T> o = hi ? v[2 * q] : v[2 * q + 1];
+    o.x = __shfl_xor_sync(0xffffffffu, o.x, 16);
+    o.y = __shfl_xor_sync(0xffffffffu, o.y, 16);
+    if (hi) v[2 * q] = o;
+    else v[2 * q + 1] = o;
+  }
+}
 // Stages s..S-1 (s >= 1); the values of stage s-1 are in v.
 template <class F, int s, int DIR, class T, class TW, class SYNC>
 __device__ __forceinline__ void fft_rest(Cx<T>* sm, int tid, Cx<T>* v, const TW& tw, SYNC sync) {
   if constexpr (s < F::S) {
-    sync();
-    fft_store<F, s - 1>(sm, tid, v);
-    sync();
-    fft_load<F, s>(sm, tid, v);
+    if constexpr (F::template halves_exchange<s>()) {
+      warp_halves_swap<F>(tid, v);
+    } else {
+      sync();
+      fft_store<F, s - 1>(sm, tid, v);
+      sync();
+      fft_load<F, s>(sm, tid, v);
+    }
     F::template compute<s, DIR>(tid, v, tw);
     fft_rest<F, s + 1, DIR>(sm, tid, v, tw, sync);
   }

@@ -16,3 +16,9 @@ def test_stockham_engine_matches_dft(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "ALL OK" in r.stdout
+    # the 512-point row transforms (16 values per thread) take their last
+    # exchange as the tid ^ 16 lane swap; no other plan does
+    for line in r.stdout.splitlines():
+        if "lane_swaps=" in line:
+            want = "lane_swaps=1" if ("L=  512 B=1 P=16" in line) else "lane_swaps=0"
+            assert want in line, line
