@@ -332,6 +332,20 @@ template <class T> struct ColFwdComArgs {
   StepArgs<T> step;
 };
 
+// Whether the column-forward pass keeps the derivative it assembles in a
+// second shared tile of CB*L values instead of registers: for CTAs of 512 or
+// more threads (128 registers per thread, one CTA per SM, so the tile costs
+// no occupancy) where both tiles fit in 160 KB; FP32 columns of up to 1024
+// points fit in registers without it.  With it the FP64 1024-point pass
+// spills 64/72 bytes per thread instead of 408/516.
+template <class T, int L, int CB, int P> __host__ __device__ constexpr bool col_fwd_com_ds() {
+  return CB * L / P >= 512 && 2 * (size_t)CB * L * sizeof(Cx<T>) <= 160 * 1024 && !(sizeof(T) == 4 && L <= 1024);
+}
+// dynamic shared memory of the column-forward pass (elements)
+template <class T, int L, int CB, int P> constexpr size_t col_fwd_com_smem_elems() {
+  return (size_t)FFTB<L, CB, P>::SMEM_ELEMS + (col_fwd_com_ds<T, L, CB, P>() ? (size_t)CB * L : 0);
+}
+
 template <class T, int L, int CB, int P>
 __global__ void __launch_bounds__(CB * L / P, TARA_MINB(CB * L / P)) k_col_fwd_com(const ColFwdComArgs<T> a) {
   using F = FFTB<L, CB, P>;
@@ -358,7 +372,7 @@ template <int L, class T>
 inline void col_fwd_com_dispatch(const ColFwdComArgs<T>& a, cudaStream_t st) {
   constexpr int CB = ColFwdComCfg<T, L>::CB, P = ColFwdComCfg<T, L>::P;
   auto kern = k_col_fwd_com<T, L, CB, P>;
-  const size_t smem = (size_t)FFTB<L, CB, P>::SMEM_ELEMS * sizeof(Cx<T>);
+  const size_t smem = col_fwd_com_smem_elems<T, L, CB, P>() * sizeof(Cx<T>);
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid((a.tb.Nh + CB - 1) / CB, 6);
   kern<<<grid, CB * L / P, smem, st>>>(a);

@@ -365,7 +365,7 @@ template <class T> size_t ens_com_col_smem() {
   size_t m = 0;
 #define TARA_EC_CS(L)                                                                                    \
   m = std::max(m, (size_t)FFTB<L, EnsComInv<T, L>::CB, EnsComInv<T, L>::P>::SMEM_ELEMS);              \
-  m = std::max(m, (size_t)FFTB<L, EnsComFwd<T, L>::CB, EnsComFwd<T, L>::P>::SMEM_ELEMS)
+  m = std::max(m, col_fwd_com_smem_elems<T, L, EnsComFwd<T, L>::CB, EnsComFwd<T, L>::P>())
   TARA_EC_CS(128);
   TARA_EC_CS(256);
   TARA_EC_CS(384);
