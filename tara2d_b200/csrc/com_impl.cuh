@@ -333,13 +333,17 @@ template <class T> struct ColFwdComArgs {
 };
 
 // Whether the column-forward pass keeps the derivative it assembles in a
-// second shared tile of CB*L values instead of registers: for CTAs of 512 or
-// more threads (128 registers per thread, one CTA per SM, so the tile costs
-// no occupancy) where both tiles fit in 160 KB; FP32 columns of up to 1024
-// points fit in registers without it.  With it the FP64 1024-point pass
-// spills 64/72 bytes per thread instead of 408/516.
+// second shared tile of CB*L values instead of registers.  Only CTAs of 512
+// or more threads (128 registers per thread, one CTA per SM, so the tile
+// costs no occupancy) where both tiles fit in 160 KB, and only where it was
+// measured no slower (graph-replayed launches, same box): FP64 1024-point
+// columns 118.7 against 118.6 us (spills 408/516 -> 64/72 bytes per thread,
+// 288 against 307 MB of DRAM traffic per launch), FP32 2048 313 against 321
+// us, FP32 4096 1650 against 1698 us.  FP64 2048-point columns were slower
+// with it (594 against 561 us) and keep the derivative in registers.
 template <class T, int L, int CB, int P> __host__ __device__ constexpr bool col_fwd_com_ds() {
-  return CB * L / P >= 512 && 2 * (size_t)CB * L * sizeof(Cx<T>) <= 160 * 1024 && !(sizeof(T) == 4 && L <= 1024);
+  return CB * L / P >= 512 && 2 * (size_t)CB * L * sizeof(Cx<T>) <= 160 * 1024 &&
+         (sizeof(T) == 8 ? L <= 1024 : L >= 2048);
 }
 // dynamic shared memory of the column-forward pass (elements)
 template <class T, int L, int CB, int P> constexpr size_t col_fwd_com_smem_elems() {
