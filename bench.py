@@ -587,7 +587,8 @@ def run_closure(args):
     """Side workload: the cost of the learned closure in the 256^2 coarse MHD
     run (FP64, RK4, dt = 1e-4, nu = eta = 1e-4, random-phase state with
     k0 = 4): device ms per RK4 step without a closure, with the closure's
-    network on tensor cores, and with it on CUDA cores; plus the network's own
+    network on tensor cores, with it on CUDA cores (both at every RK4 stage),
+    and on tensor cores once per step; plus the network's own
     device time per 256^2 field (forward; forward + backward).  The network's
     parameters are seeded random values (the cost does not depend on them)."""
     import numpy as np
@@ -606,11 +607,13 @@ def run_closure(args):
         res["cnn_tc_ms"] = c.time_cnn(1, 20)
         c.set_tensor_cores(False)
         res["cnn_cuda_ms"] = c.time_cnn(1, 20)
-        for mode in ("none", "tensor_cores", "cuda_cores"):
+        for mode in ("none", "tensor_cores", "cuda_cores", "tensor_cores_once"):
             with T.Session(T.MODEL_COM, N, N, T.Params.make(**kw)) as s:
                 s.set_state(st)
                 if mode != "none":
-                    c.set_tensor_cores(mode == "tensor_cores")
+                    c.set_tensor_cores(mode != "cuda_cores")
+                    s.set_closure_mode(T.CLOSURE_ONCE_PER_STEP if mode == "tensor_cores_once"
+                                       else T.CLOSURE_EVERY_RHS)
                     T.attach_closure(s, c)
                 s.step(T.STEP_RK4, W)
                 res[mode] = s.time_steps(T.STEP_RK4, K) / K
@@ -621,8 +624,10 @@ def run_closure(args):
                                   "5->32->32->32->4 (3x3, GELU), seeded random parameters"},
            "unclosed_ms_per_step": res["none"], "closed_tensor_cores_ms_per_step": res["tensor_cores"],
            "closed_cuda_cores_ms_per_step": res["cuda_cores"],
+           "closed_tensor_cores_once_per_step_ms_per_step": res["tensor_cores_once"],
            "closed_over_unclosed": {"tensor_cores": res["tensor_cores"] / res["none"],
-                                    "cuda_cores": res["cuda_cores"] / res["none"]},
+                                    "cuda_cores": res["cuda_cores"] / res["none"],
+                                    "tensor_cores_once_per_step": res["tensor_cores_once"] / res["none"]},
            "cnn_ms_per_field": {"tensor_cores": {"forward": res["cnn_tc_ms"][0], "forward_backward": res["cnn_tc_ms"][1]},
                                 "cuda_cores": {"forward": res["cnn_cuda_ms"][0],
                                                "forward_backward": res["cnn_cuda_ms"][1]}}}

@@ -289,6 +289,16 @@ int tara_closure_status(tara_closure* c);
  * forward + backward. */
 int tara_closure_time_cnn(tara_closure* c, int B, int reps, float* ms_forward, float* ms_backward);
 int tara_session_attach_closure(tara_session* s, tara_closure* c); /* c = NULL detaches */
+/* Where an attached closure is evaluated in RK4 steps.
+ * TARA_CLOSURE_EVERY_RHS (the default): every RHS evaluation, each RK4 stage
+ * with the closure of its own input.  TARA_CLOSURE_ONCE_PER_STEP: at the
+ * first stage of each step only; stages 2-4 reuse its stress/EMF spectra
+ * (first order in time for the subgrid term, a quarter of its cost).  AB2,
+ * Euler and single RHS calls evaluate it once per RHS in both modes.  Holds
+ * across detach/attach; TARA_EINVAL for another mode value. */
+#define TARA_CLOSURE_EVERY_RHS 0
+#define TARA_CLOSURE_ONCE_PER_STEP 1
+int tara_session_set_closure_mode(tara_session* s, int mode);
 int tara_filter_state(tara_session* fine, tara_session* coarse);
 
 /* ---- batched ensembles (no counterpart in the reference, whose drivers run

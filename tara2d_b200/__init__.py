@@ -25,6 +25,7 @@ CFL_OFF, CFL_CHECK, CFL_ADAPT = 0, 1, 2
 MODEL_COH, MODEL_COM, MODEL_CSH, MODEL_CSS = 1, 2, 3, 4
 FP64, FP32 = 0, 1
 STEP_AB2, STEP_RK4, STEP_EULER = 0, 1, 2
+CLOSURE_EVERY_RHS, CLOSURE_ONCE_PER_STEP = 0, 1
 LEGACY_REFERENCE, LEGACY_CORRECT = 0, 1
 SUPPORTED_N = (16, 32, 64, 128, 256, 384, 512, 1024, 2048, 4096)
 NUM_KERNEL_KINDS = 12
@@ -123,6 +124,7 @@ def lib():
         L.tara_closure_status.argtypes = [P]
         L.tara_closure_time_cnn.argtypes = [P, I, I, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.tara_session_attach_closure.argtypes = [P, P]
+        L.tara_session_set_closure_mode.argtypes = [P, C.c_int]
         L.tara_filter_state.argtypes = [P, P]
         L.tara_get_state_real.argtypes = [P, PP]
         L.tara_set_state_real.argtypes = [P, PP]
@@ -336,6 +338,12 @@ class Session:
     def set_cfl(self, mode: int, cfl: float = 0.0) -> None:
         """CFL control (CFL_OFF, CFL_CHECK, CFL_ADAPT) with CFL number cfl."""
         check(lib().tara_set_cfl(self._h, mode, cfl), "tara_set_cfl")
+
+    def set_closure_mode(self, mode: int) -> None:
+        """Where an attached closure is evaluated in RK4 steps:
+        CLOSURE_EVERY_RHS (default) or CLOSURE_ONCE_PER_STEP (stages 2-4
+        reuse the first stage's subgrid spectra)."""
+        check(lib().tara_session_set_closure_mode(self._h, mode), "tara_session_set_closure_mode")
 
     def time(self):
         """(model time advanced so far, dt of the last step)."""

@@ -309,7 +309,9 @@ struct SessionT : tara_session {
         return coh_rhs(g, cw, cohp, in, s, st);
       case TARA_MODEL_COM: {
         if constexpr (sizeof(T) == sizeof(double)) {
-          if (clos) {  // the learned closure's stress/EMF spectra for this RHS input
+          // the learned closure's stress/EMF spectra for this RHS input; once
+          // per step, RK4 stages 1-3 keep those of stage 0
+          if (clos && (clos_mode == TARA_CLOSURE_EVERY_RHS || s.mode != STEP_RK4 || s.stage == 0)) {
             Cx<double>* out4[4] = {closf[0], closf[1], closf[2], closf[3]};
             TARA_TRY(closure_terms(clos, g, in, out4, st));
           }
@@ -335,7 +337,17 @@ struct SessionT : tara_session {
 
   // learned closure (MHD, FP64 sessions of the closure's coarse grid)
   tara_closure* clos = nullptr;
+  int clos_mode = TARA_CLOSURE_EVERY_RHS;
   FieldPool<T> closf;
+  int set_closure_mode(int mode) override {
+    if (mode != TARA_CLOSURE_EVERY_RHS && mode != TARA_CLOSURE_ONCE_PER_STEP) {
+      set_error("closure mode must be TARA_CLOSURE_EVERY_RHS or TARA_CLOSURE_ONCE_PER_STEP");
+      return TARA_EINVAL;
+    }
+    if (mode != clos_mode) drop_graphs();  // captured steps hold the closure launches of the old mode
+    clos_mode = mode;
+    return TARA_OK;
+  }
   const void* grid_ptr() const override { return &g; }
   void* state_ptr(int q) override { return q >= 0 && q < nf ? (void*)u[q] : nullptr; }
   int attach_closure(tara_closure* c) override {

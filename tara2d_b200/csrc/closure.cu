@@ -525,6 +525,10 @@ int tara_session_attach_closure(tara_session* s, tara_closure* c) {
   if (!s) return TARA_EINVAL;
   return s->fail_if(s->attach_closure(c));
 }
+int tara_session_set_closure_mode(tara_session* s, int mode) {
+  if (!s) return TARA_EINVAL;
+  return s->fail_if(s->set_closure_mode(mode));
+}
 // coarse state = sharp spectral filter of the fine state (both MHD FP64)
 int tara_filter_state(tara_session* fine, tara_session* coarse) {
   if (!fine || !coarse) return TARA_EINVAL;

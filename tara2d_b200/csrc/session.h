@@ -61,6 +61,7 @@ struct tara_session {
   virtual const void* grid_ptr() const = 0;
   virtual void* state_ptr(int q) = 0;
   virtual int attach_closure(tara_closure* c) = 0;
+  virtual int set_closure_mode(int mode) = 0;  // TARA_CLOSURE_*
   // the state was changed from outside the stepping kernels: drop what was
   // derived from it
   virtual void invalidate_derived() = 0;

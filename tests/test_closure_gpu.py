@@ -179,3 +179,93 @@ def test_training_reduces_the_loss(tara):
         after = c.eval_loss(0, 24)
     assert np.all(np.isfinite(losses))
     assert after < 0.5 * before, (before, after, losses[-5:])
+
+
+def _rk4_host(s, u0, dt, term):
+    """One classical RK4 step built from single RHS calls of session `s`
+    (closure detached): k_i = rhs(stage input) + term(stage index, input)."""
+    def f(i, u):
+        s.set_state(u)
+        r = s.rhs()
+        t = term(i, u)
+        return [a + b for a, b in zip(r, t)]
+    k1 = f(0, u0)
+    k2 = f(1, [a + 0.5 * dt * b for a, b in zip(u0, k1)])
+    k3 = f(2, [a + 0.5 * dt * b for a, b in zip(u0, k2)])
+    k4 = f(3, [a + dt * b for a, b in zip(u0, k3)])
+    return [a + dt / 6.0 * (b + 2.0 * c + 2.0 * d + e) for a, b, c, d, e in zip(u0, k1, k2, k3, k4)]
+
+
+@pytest.mark.parametrize("mode", ["every_rhs", "once_per_step"])
+def test_closure_mode_in_rk4_steps(tara, mode):
+    """An RK4 step with the closure attached against the classical RK4 step
+    built on the host from single RHS evaluations: every RHS evaluation adds
+    the closure term of its own stage input (CLOSURE_EVERY_RHS), or all four
+    stages add the term of the step's input (CLOSURE_ONCE_PER_STEP).  The
+    step increments agree to relative L2 <= 1e-9 per field (FP64; the fused
+    stepper rounds in another order), the two modes differ by far more than
+    that, and four captured single steps equal one call of four steps."""
+    N, dt = 32, 2e-4
+    st = compressive(I.com_random_phase(N, N, seed=9), 3)
+    norm = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 1e-3, 0.3, 0.3, 0.4, 0.4,
+                     1e-3, -2e-3, 5e-4, 1e-4, 2e-2, 1e-2, 3e-2, 5e-3], np.float32)
+    want = tara.CLOSURE_EVERY_RHS if mode == "every_rhs" else tara.CLOSURE_ONCE_PER_STEP
+    with tara.Session(tara.MODEL_COM, N, N, tara.Params.make(**com_kw(dt=dt))) as s, tara.Closure(N, 1) as c:
+        c.set_params(_random_params(tara, 5, 0.2))
+        c.set_norm(norm)
+
+        def closure_term(u):
+            s.set_state(u)
+            plain = s.rhs()
+            tara.attach_closure(s, c)
+            closed = s.rhs()
+            tara.attach_closure(s, None)
+            return [a - b for a, b in zip(closed, plain)]
+
+        c0 = closure_term(st)
+        ref = {"every_rhs": _rk4_host(s, st, dt, lambda i, u: closure_term(u)),
+               "once_per_step": _rk4_host(s, st, dt, lambda i, u: c0)}
+        s.set_closure_mode(want)
+        tara.attach_closure(s, c)
+        s.set_state(st)
+        s.step(tara.STEP_RK4, 1)
+        got = s.get_state()
+        s.set_state(st)
+        for _ in range(4):
+            s.step(tara.STEP_RK4, 1)
+        four_single = s.get_state()
+        s.set_state(st)
+        s.step(tara.STEP_RK4, 4)
+        four = s.get_state()
+        with pytest.raises(tara.TaraError):
+            s.set_closure_mode(2)
+        tara.attach_closure(s, None)
+    other = "once_per_step" if mode == "every_rhs" else "every_rhs"
+    for f in (1, 2, 4, 5):  # the fields the closure acts on
+        inc = got[f] - st[f]
+        err = rel_l2(inc, ref[mode][f] - st[f])
+        gap = rel_l2(ref[other][f] - st[f], ref[mode][f] - st[f])
+        assert err <= 1e-9, (f, err)
+        assert gap > 1e3 * max(err, 1e-12), (f, err, gap)
+    for a, b in zip(four_single, four):
+        assert np.array_equal(a, b)
+
+
+def test_closure_mode_leaves_ab2_unchanged(tara):
+    """AB2 has one RHS evaluation per step: both closure modes give the same
+    bits."""
+    N = 32
+    st = compressive(I.com_random_phase(N, N, seed=11), 3)
+    out = []
+    with tara.Closure(N, 1) as c:
+        c.set_params(_random_params(tara, 6, 0.2))
+        for mode in (tara.CLOSURE_EVERY_RHS, tara.CLOSURE_ONCE_PER_STEP):
+            with tara.Session(tara.MODEL_COM, N, N, tara.Params.make(**com_kw())) as s:
+                s.set_closure_mode(mode)
+                tara.attach_closure(s, c)
+                s.set_state(st)
+                s.step(tara.STEP_AB2, 5)
+                out.append(s.get_state() + s.get_history())
+                tara.attach_closure(s, None)
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
