@@ -8,6 +8,9 @@ train: for each training seed, an FP64 MHD DNS on N x N (nu = eta = 1e-4,
 CS = 100, random-phase u and B with E(k) ~ k^4 exp(-(k/k0)^2)) is spun up and
 then sampled every `--pair-every` steps; each sample is sharp-filtered to
 Nc x Nc and turned into an (input, subgrid stress/EMF) pair on the device.
+With `--ensemble M` the pairs come instead from M fine runs (N <= 512)
+stepped together as one batched ensemble (AB2 at `--ensemble-dt`, sampled at
+the same model times), one pair per member per sample, until `--capacity`.
 The CNN is trained on the pairs and saved with its normalisation to
 DIR/closure_model.npz.
 
@@ -44,18 +47,47 @@ def dns_session(N, seed, k0, nu, dt):
     return s
 
 
+def ensemble_pairs(a, c):
+    """Training pairs from an FP64 MHD ensemble of `a.ensemble` fine runs
+    (seeds train_seeds[0], train_seeds[0] + 1, ...) stepped together by AB2
+    at dt = `a.ensemble_dt` (ensembles step with AB2; at CS = 100 AB2 needs a
+    smaller dt than RK4), spun up and sampled at the model times of the
+    RK4 schedule; each sample gives one pair per member.  Returns the
+    ensemble's AB2 steps."""
+    from . import STEP_AB2, Ensemble
+    M = a.ensemble
+    spin = max(1, round(a.spin_steps * a.dt / a.ensemble_dt))
+    every = max(1, round(a.pair_every * a.dt / a.ensemble_dt))
+    steps = 0
+    with Ensemble([a.n] * M, params(a.nu, a.ensemble_dt), precision=FP64, model=MODEL_COM) as e:
+        for m in range(M):
+            e.set_state(m, initial.com_random_phase(a.n, a.n, seed=a.train_seeds[0] + m, k0=a.k0))
+        e.step(STEP_AB2, spin)
+        steps += spin
+        while c.count + M <= a.capacity:
+            e.step(STEP_AB2, every)
+            steps += every
+            for m in range(M):
+                c.add_pair_member(e, m)
+    return steps
+
+
 def train(a):
     c = Closure(a.nc, a.capacity, batch_max=a.batch, seed=a.seed)
     t0 = time.time()
     dns_ms = 0.0
-    for seed in a.train_seeds:
-        with dns_session(a.n, seed, a.k0, a.nu, a.dt) as s:
-            dns_ms += s.time_steps(STEP_RK4, a.spin_steps)
-            for _ in range(a.pairs_per_seed):
-                if c.count >= a.capacity:
-                    break
-                dns_ms += s.time_steps(STEP_RK4, a.pair_every)
-                c.add_pair(s)
+    ens_steps = 0
+    if a.ensemble:
+        ens_steps = ensemble_pairs(a, c)
+    else:
+        for seed in a.train_seeds:
+            with dns_session(a.n, seed, a.k0, a.nu, a.dt) as s:
+                dns_ms += s.time_steps(STEP_RK4, a.spin_steps)
+                for _ in range(a.pairs_per_seed):
+                    if c.count >= a.capacity:
+                        break
+                    dns_ms += s.time_steps(STEP_RK4, a.pair_every)
+                    c.add_pair(s)
     npairs = c.count
     nval = max(1, npairs // 10)
     ntrain = npairs - nval
@@ -73,6 +105,8 @@ def train(a):
     val1 = c.eval_loss(ntrain, nval)
     np.savez(os.path.join(a.out, "closure_model.npz"), params=c.get_params(), norm=c.get_norm())
     rep = {"pairs": npairs, "train_pairs": ntrain, "validation_pairs": nval, "grid": [a.n, a.nc],
+           "source": f"ensemble of {a.ensemble} members, AB2 dt {a.ensemble_dt}" if a.ensemble else "sessions",
+           "ensemble_steps": ens_steps,
            "dns_device_s": dns_ms / 1e3, "data_wall_s": t1 - t0, "train_wall_s": t2 - t1, "epochs": a.epochs,
            "loss_before": loss0, "validation_before": val0, "epoch_loss": losses, "validation_after": val1}
     with open(os.path.join(a.out, "closure_train.json"), "w") as f:
@@ -162,6 +196,9 @@ def main(argv=None):
     ap.add_argument("--pair-every", type=int, default=25)
     ap.add_argument("--pairs-per-seed", type=int, default=400)
     ap.add_argument("--capacity", type=int, default=800)
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="train: take the pairs from an ensemble of this many fine runs (N <= 512)")
+    ap.add_argument("--ensemble-dt", type=float, default=1e-5, help="AB2 time step of the ensemble runs")
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=2e-3)
