@@ -120,6 +120,9 @@ int main() {
   BOTH(16, 4, 16) BOTH(32, 1, 16) BOTH(64, 8, 16) BOTH(128, 8, 16) BOTH(256, 4, 16) BOTH(512, 4, 16) BOTH(512, 1, 16)
   BOTH(1024, 4, 16) BOTH(2048, 2, 16) BOTH(4096, 1, 16)
   BOTH(48, 2, 24) BOTH(96, 1, 24) BOTH(192, 1, 24) BOTH(384, 4, 24) BOTH(768, 1, 24)
+  // the column tiles the MHD column-forward pass runs (kx columns x values per thread)
+  BOTH(256, 8, 16) BOTH(512, 2, 8) BOTH(512, 4, 8) BOTH(1024, 4, 8) BOTH(2048, 2, 8) BOTH(2048, 4, 8)
+  BOTH(4096, 2, 8) BOTH(4096, 2, 16)
   printf("%s\n", fails ? "FAILED" : "ALL OK");
   return fails ? 1 : 0;
 }
